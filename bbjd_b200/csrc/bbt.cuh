@@ -1,0 +1,70 @@
+// Device-resident block-bordered (BBT) pencil and its preconditioners.
+#pragma once
+
+#include <vector>
+
+#include "dense.cuh"
+
+struct bbjd_precond;
+
+struct bbjd_bbt_matrix {
+    int b = 0, t = 0;
+    int64_t nblk = 0, nb = 0, n = 0;
+    bbjd::cplx *Ad = nullptr, *Al = nullptr, *Au = nullptr, *Bd = nullptr;  // [nblk][b*b] col-major
+    bbjd::cplx *E = nullptr;   // nb x t col-major
+    bbjd::cplx *FT = nullptr;  // n x t row-major == F (t x n) col-major
+    bbjd::cplx *mem = nullptr;
+    // scratch of the fused product
+    int G = 0;
+    bbjd::cplx *tau_part = nullptr;  // [G][t]
+    double *rn_part = nullptr;       // [G]
+    double *rnorm = nullptr;         // device scalar: ||r|| of the last residual product
+};
+
+namespace bbjd {
+
+// yA = A x, yB = B x; if r != nullptr also r = tb*yA - ta*yB and
+// *rnorm = ||r|| (device; m->rnorm when null).  One pass over the pencil's
+// storage.  The product's scratch lives in the matrix: one product at a time
+// per matrix.
+bbjd_status bbt_apply(const bbjd_bbt_matrix *m, const cplx *x, cplx *yA, cplx *yB, cplx ta,
+                      cplx tb, cplx *r, double *rnorm, cudaStream_t st);
+bbjd_status precond_solve(const bbjd_precond *pc, int nrhs, const cplx *r, cplx *x, int64_t stride,
+                          cudaStream_t st);
+double precond_bytes(const bbjd_precond *pc, int nrhs);
+
+double bbt_bytes(const bbjd_bbt_matrix *m, bool with_residual);
+
+}  // namespace bbjd
+
+struct bbjd_precond {
+    int kind = 0, precision = 0;
+    int b = 0, t = 0;
+    int64_t nblk = 0, nb = 0, n = 0;
+    // block cyclic reduction of the block-tridiagonal interior
+    struct Level {
+        int64_t N = 0, n_odd = 0, n_even = 0;
+        bbjd::cplx *Dinv = nullptr, *DinvLo = nullptr, *DinvUp = nullptr;  // n_odd blocks
+        bbjd::cplx *Alpha = nullptr, *Beta = nullptr;                      // n_even blocks
+        int64_t vec_off = 0;  // offset of this level's compact vectors in lvl_rhs / lvl_x
+    };
+    std::vector<Level> levels;
+    bbjd::cplx *Dinv_top = nullptr;
+    bbjd::cplx *pool = nullptr;     // all factor blocks
+    // border (t > 0): Y = K^-1 E (nb x t col-major), Sinv = (G - F1 Y)^-1 (t x t)
+    bbjd::cplx *Y = nullptr;
+    bbjd::cplx *Sinv = nullptr;
+    const bbjd::cplx *FT = nullptr; // borrowed from the matrix
+    // block Jacobi: Dinv for every block, Ginv for the tau corner
+    bbjd::cplx *Ginv = nullptr;
+    // solve scratch
+    bbjd::cplx *lvl_rhs = nullptr, *lvl_x = nullptr;   // 2 RHS x (sum of level sizes)
+    int64_t lvl_total = 0;
+    int64_t top_off = 0;
+    int G = 0;
+    bbjd::cplx *tau_part = nullptr;  // [G][2][t]
+    bbjd::cplx *x2 = nullptr;        // [2][t]
+    int *err = nullptr;              // device: singular pivot seen
+    double factor_seconds = 0.0;
+    double min_pivot = 0.0;
+};

@@ -1,0 +1,497 @@
+// Tall-skinny dense kernels of the JDQZ iteration (FP64 complex, sm_100a).
+//
+// Replaces the OpenBLAS calls the reference makes on n-row data:
+//   zgemv 'C' / 'N' + dznrm2 of CGS2/DGKS  (reference jd_core.c:207-241)
+//   zgemv 'N' Ritz vector u = V x          (reference jd_core.c:870-877)
+//   zgemv 'C' + zdotc pencil column/row    (reference jd_core.c:1085-1104)
+//   zdotc + zaxpy SvdV step                (reference jd_core.c:966-971)
+//   zgemm restart V*ZB, AV*ZB, BV*ZB       (reference jd_core.c:989-999)
+//   zgemm W^H AV, W^H BV                   (reference jd_core.c:1020-1025)
+//
+// All are HBM-bound except the restart/Gram GEMMs (FP64 FMA-bound).  Every
+// reduction is two-stage with a fixed summation order, so results do not
+// depend on scheduling.
+#include "dense.cuh"
+
+#include <algorithm>
+#include <cstdio>
+
+namespace bbjd {
+
+// ---------------------------------------------------------------------------
+// Stage 1 of Q^H v: partial[g][x] for x = (m*NV + p)*ncols + j, plus the
+// squared norms of the vectors at x = NM*NV*ncols + p.
+// One CTA owns a contiguous row range; its slice of each vector is staged in
+// shared memory once; warp w streams columns j = w, w + nwarps, ... of Q.
+template <int NM, int NV>
+__global__ void __launch_bounds__(256) k_tsdot(int64_t n, int ncols, int64_t ld,
+                                               const cplx *__restrict__ Q0,
+                                               const cplx *__restrict__ Q1,
+                                               const cplx *__restrict__ v0,
+                                               const cplx *__restrict__ v1, int64_t rpc,
+                                               cplx *__restrict__ partial, const int *flag) {
+    if (flag && *flag == 0) return;
+    extern __shared__ cplx sv[];
+    const int64_t r0 = (int64_t)blockIdx.x * rpc;
+    const int64_t r1 = min(n, r0 + rpc);
+    const int nr = (int)max((int64_t)0, r1 - r0);
+    const int X = NM * NV * ncols + NV;
+    cplx *out = partial + (int64_t)blockIdx.x * X;
+
+    double nsq[NV];
+#pragma unroll
+    for (int p = 0; p < NV; ++p) nsq[p] = 0.0;
+    for (int i = threadIdx.x; i < nr; i += blockDim.x) {
+        cplx a = v0[r0 + i];
+        sv[i] = a;
+        nsq[0] += cabs2(a);
+        if (NV > 1) {
+            cplx b = v1[r0 + i];
+            sv[rpc + i] = b;
+            nsq[NV - 1] += cabs2(b);
+        }
+    }
+    __shared__ double snorm[NV][8];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+#pragma unroll
+    for (int p = 0; p < NV; ++p) {
+        double s = warp_sum(nsq[p]);
+        if (lane == 0) snorm[p][warp] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x < NV) {
+        double s = 0.0;
+        for (int w = 0; w < nwarps; ++w) s += snorm[threadIdx.x][w];
+        out[NM * NV * ncols + threadIdx.x] = mk(s, 0.0);
+    }
+
+    for (int cj = warp; cj < NM * ncols; cj += nwarps) {
+        const int m = cj / ncols, j = cj - m * ncols;
+        const cplx *q = ((NM > 1 && m == 1) ? Q1 : Q0) + (int64_t)j * ld + r0;
+        cplx acc[NV];
+#pragma unroll
+        for (int p = 0; p < NV; ++p) acc[p] = mk(0.0, 0.0);
+        int i = lane;
+        for (; i + 96 < nr; i += 128) {
+            cplx q0 = ldg_stream(q + i), q1 = ldg_stream(q + i + 32);
+            cplx q2 = ldg_stream(q + i + 64), q3 = ldg_stream(q + i + 96);
+#pragma unroll
+            for (int p = 0; p < NV; ++p) {
+                const cplx *s = sv + p * rpc;
+                cfmac(acc[p], q0, s[i]);
+                cfmac(acc[p], q1, s[i + 32]);
+                cfmac(acc[p], q2, s[i + 64]);
+                cfmac(acc[p], q3, s[i + 96]);
+            }
+        }
+        for (; i < nr; i += 32) {
+            cplx qv = ldg_stream(q + i);
+#pragma unroll
+            for (int p = 0; p < NV; ++p) cfmac(acc[p], qv, sv[p * rpc + i]);
+        }
+#pragma unroll
+        for (int p = 0; p < NV; ++p) {
+            cplx s = warp_sum(acc[p]);
+            if (lane == 0) out[(m * NV + p) * ncols + j] = s;
+        }
+    }
+}
+
+// Stage 2: out[x] = sum_g partial[g][x] in a fixed order.
+__global__ void __launch_bounds__(256) k_reduce(const cplx *__restrict__ partial, int G, int X,
+                                                cplx *__restrict__ out, const int *flag) {
+    if (flag && *flag == 0) return;
+    __shared__ cplx s[8][33];
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const int x = blockIdx.x * 32 + tx;
+    cplx acc = mk(0.0, 0.0);
+    if (x < X)
+        for (int g = ty; g < G; g += 8) acc = cadd(acc, partial[(int64_t)g * X + x]);
+    s[ty][tx] = acc;
+    __syncthreads();
+    if (ty == 0 && x < X) {
+        cplx r = s[0][tx];
+        for (int k = 1; k < 8; ++k) r = cadd(r, s[k][tx]);
+        out[x] = r;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// v_out = a v_in + b w_in - Q (c1 h1 + c2 h2), and ||v_out||.
+// The last CTA to finish sums the per-CTA squared norms in a fixed order,
+// stores the norm, and (optionally) raises the DGKS flag
+//   flag_out = ||v_out|| < 0.7071 ||v_before||       (reference jd_core.c:232)
+// where ||v_before||^2 is read from ref_nsq (the x = NM*NV*ncols slot the
+// first-pass dot kernel wrote).
+__global__ void __launch_bounds__(256) k_update(
+    int64_t n, int ncols, int64_t ld, const cplx *__restrict__ Q, const cplx *__restrict__ h1,
+    const cplx *__restrict__ h2, cplx c1, cplx c2, cplx a, const cplx *v_in, cplx b,
+    const cplx *__restrict__ w_in, cplx *v_out, double *__restrict__ nrm_part,
+    unsigned *counter, double *norm_out, const cplx *ref_nsq, const double *ref_nrm, int *flag_out,
+    const int *flag_in) {
+    if (flag_in && *flag_in == 0) return;
+    extern __shared__ cplx hs[];
+    for (int j = threadIdx.x; j < ncols; j += blockDim.x) {
+        cplx h = cmul(c1, h1[j]);
+        if (h2) cfma(h, c2, h2[j]);
+        hs[j] = h;
+    }
+    __syncthreads();
+    double nsq = 0.0;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        cplx acc = mk(0.0, 0.0);
+        if (v_in) acc = cmul(a, v_in[i]);
+        if (w_in) cfma(acc, b, w_in[i]);
+        const cplx *q = Q + i;
+        int j = 0;
+        for (; j + 8 <= ncols; j += 8) {
+            cplx qv[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) qv[u] = ldg_stream(q + (int64_t)(j + u) * ld);
+#pragma unroll
+            for (int u = 0; u < 8; ++u) cfms(acc, qv[u], hs[j + u]);
+        }
+        for (; j < ncols; ++j) cfms(acc, ldg_stream(q + (int64_t)j * ld), hs[j]);
+        v_out[i] = acc;
+        nsq += cabs2(acc);
+    }
+    __shared__ double red[8];
+    __shared__ bool last;
+    double s = warp_sum(nsq);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+        nrm_part[blockIdx.x] = t;
+        __threadfence();
+        last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    double t = 0.0;
+    for (int g = threadIdx.x; g < (int)gridDim.x; g += blockDim.x) t += __ldcg(nrm_part + g);
+    t = warp_sum(t);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = t;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double tot = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += red[w];
+        const double nrm = sqrt(tot);
+        *norm_out = nrm;
+        if (flag_out) {
+            const double before = ref_nsq ? sqrt(ref_nsq->x) : (ref_nrm ? *ref_nrm : 0.0);
+            *flag_out = (nrm < 0.7071 * before) ? 1 : 0;
+        }
+        *counter = 0u;
+    }
+}
+
+// out = v / norm (norm read on the device); if norm <= thresh, out = v.
+__global__ void k_scale(int64_t n, const cplx *v, const double *norm, double thresh, cplx *out) {
+    const double nr = *norm;
+    const double s = nr > thresh ? 1.0 / nr : 1.0;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        out[i] = cscale(v[i], s);
+}
+
+// out = a x + b y with device-resident complex coefficients.
+__global__ void k_axpby(int64_t n, const cplx *a_dev, cplx a_host, const cplx *x,
+                        const cplx *b_dev, cplx b_host, const cplx *y, cplx *out) {
+    const cplx a = a_dev ? *a_dev : a_host;
+    const cplx b = b_dev ? *b_dev : b_host;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        cplx r = cmul(a, x[i]);
+        if (y) cfma(r, b, y[i]);
+        out[i] = r;
+    }
+}
+
+// SvdV step (reference jd_core.c:966-971): dots = [u^H z, u^H s] from the
+// reduce kernel; out = z - s (u^H z)/(u^H s) when |u^H s| > 1e-300, else z.
+__global__ void k_svdv(int64_t n, const cplx *__restrict__ dots, const cplx *__restrict__ z,
+                       const cplx *__restrict__ s, cplx *__restrict__ out) {
+    const cplx uz = dots[0], us = dots[1];
+    const double den = cabs2(us);
+    cplx coeff = mk(0.0, 0.0);
+    if (sqrt(den) > 1e-300) {
+        // -(uz / us)
+        coeff = mk(-(uz.x * us.x + uz.y * us.y) / den, -(uz.y * us.x - uz.x * us.y) / den);
+    }
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        cplx r = z[i];
+        cfma(r, coeff, s[i]);
+        out[i] = r;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Restart compression out[:, 0:keep] = X[:, 0:k] Z[0:k, 0:keep] (FP64).
+// A CTA owns 64 rows; the k x keep coefficient block Z is read from L2
+// through 32-row K-slices staged in shared memory.  Each thread holds a
+// 4 x RC register tile.  The CTA writes its rows only after it has read all
+// of X's columns for them, so out may alias X (in-place restart, no swap
+// buffer and no copy-back as in reference jd_core.c:991-999).
+constexpr int RG_ROWS = 64, RG_KS = 16;
+template <int RC>
+__global__ void __launch_bounds__(256) k_restart_gemm(int64_t n, int k, int keep,
+                                                      const cplx *X, int64_t ldx,
+                                                      const cplx *__restrict__ Z, int ldz,
+                                                      cplx *out) {
+    // thread layout: 16 row-groups x 16 column-groups; rows r = rg + 16*u (u<4),
+    // columns c = cg + 16*v (v < RC) -> covers 64 rows x 16*RC columns.
+    __shared__ cplx sX[RG_KS][RG_ROWS];
+    __shared__ cplx sZ[RG_KS][16 * RC];
+    const int tid = threadIdx.x, rg = tid & 15, cg = tid >> 4;
+    const int64_t row0 = (int64_t)blockIdx.x * RG_ROWS;
+    const int colbase = blockIdx.y * 16 * RC;
+    cplx acc[4][RC];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < RC; ++v) acc[u][v] = mk(0.0, 0.0);
+
+    for (int j0 = 0; j0 < k; j0 += RG_KS) {
+        for (int e = tid; e < RG_KS * RG_ROWS; e += 256) {
+            const int jj = e / RG_ROWS, rr = e - jj * RG_ROWS;
+            const int64_t row = row0 + rr;
+            sX[jj][rr] = (j0 + jj < k && row < n) ? X[(int64_t)(j0 + jj) * ldx + row] : mk(0.0, 0.0);
+        }
+        for (int e = tid; e < RG_KS * 16 * RC; e += 256) {
+            const int jj = e % RG_KS, cc = e / RG_KS;
+            const int col = colbase + cc;
+            sZ[jj][cc] = (j0 + jj < k && col < keep) ? Z[(int64_t)col * ldz + j0 + jj] : mk(0.0, 0.0);
+        }
+        __syncthreads();
+#pragma unroll 4
+        for (int jj = 0; jj < RG_KS; ++jj) {
+            cplx xv[4], zv[RC];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) xv[u] = sX[jj][rg + 16 * u];
+#pragma unroll
+            for (int v = 0; v < RC; ++v) zv[v] = sZ[jj][cg + 16 * v];
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int v = 0; v < RC; ++v) cfma(acc[u][v], xv[u], zv[v]);
+        }
+        __syncthreads();
+    }
+    // every CTA of this row block must finish reading X before any writes
+    // when out aliases X: the grid's y dimension splits columns, so the
+    // in-place form is only used with gridDim.y == 1 (checked on the host).
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const int64_t row = row0 + rg + 16 * u;
+        if (row >= n) continue;
+#pragma unroll
+        for (int v = 0; v < RC; ++v) {
+            const int col = colbase + cg + 16 * v;
+            if (col < keep) out[(int64_t)col * ldx + row] = acc[u][v];
+        }
+    }
+}
+
+// Gram stage 1: partial[g] (keep x keep, column-major) = X_g^H Y_g over the
+// CTA's row range.  Each thread holds a 5 x 5 tile (keep <= 80 per launch
+// tile; larger keep tiles over blockIdx.y / z).
+constexpr int GR_T = 80, GR_SUB = 16;
+__global__ void __launch_bounds__(256) k_gram(int64_t n, int keep, const cplx *__restrict__ X,
+                                              const cplx *__restrict__ Y, int64_t ldx,
+                                              int64_t rpc, cplx *__restrict__ partial) {
+    __shared__ cplx sX[GR_SUB][GR_T];
+    __shared__ cplx sY[GR_SUB][GR_T];
+    const int tid = threadIdx.x, ta = tid & 15, tb = tid >> 4;
+    const int a0 = blockIdx.y * GR_T, b0 = blockIdx.z * GR_T;
+    const int64_t r0 = (int64_t)blockIdx.x * rpc, r1 = min(n, r0 + rpc);
+    cplx acc[5][5];
+#pragma unroll
+    for (int u = 0; u < 5; ++u)
+#pragma unroll
+        for (int v = 0; v < 5; ++v) acc[u][v] = mk(0.0, 0.0);
+    for (int64_t rs = r0; rs < r1; rs += GR_SUB) {
+        for (int e = tid; e < GR_SUB * GR_T; e += 256) {
+            const int c = e / GR_SUB, rr = e - c * GR_SUB;
+            const int64_t row = rs + rr;
+            const bool ok = row < r1;
+            sX[rr][c] = (ok && a0 + c < keep) ? X[(int64_t)(a0 + c) * ldx + row] : mk(0.0, 0.0);
+            sY[rr][c] = (ok && b0 + c < keep) ? Y[(int64_t)(b0 + c) * ldx + row] : mk(0.0, 0.0);
+        }
+        __syncthreads();
+#pragma unroll 4
+        for (int rr = 0; rr < GR_SUB; ++rr) {
+            cplx xv[5], yv[5];
+#pragma unroll
+            for (int u = 0; u < 5; ++u) xv[u] = sX[rr][ta + 16 * u];
+#pragma unroll
+            for (int v = 0; v < 5; ++v) yv[v] = sY[rr][tb + 16 * v];
+#pragma unroll
+            for (int u = 0; u < 5; ++u)
+#pragma unroll
+                for (int v = 0; v < 5; ++v) cfmac(acc[u][v], xv[u], yv[v]);
+        }
+        __syncthreads();
+    }
+    cplx *out = partial + (int64_t)blockIdx.x * keep * keep;
+#pragma unroll
+    for (int u = 0; u < 5; ++u) {
+        const int a = a0 + ta + 16 * u;
+        if (a >= keep) continue;
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+            const int bb = b0 + tb + 16 * v;
+            if (bb < keep) out[(int64_t)bb * keep + a] = acc[u][v];
+        }
+    }
+}
+
+// ===========================================================================
+// Host wrappers
+// ===========================================================================
+
+std::atomic<long long> g_launches{0};
+
+int num_sms() {
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 148;
+    }
+    return sms;
+}
+
+static thread_local char g_errbuf[512];
+void set_last_error(cudaError_t e, const char *what, const char *file, int line) {
+    snprintf(g_errbuf, sizeof(g_errbuf), "%s: %s (%s:%d)", what, cudaGetErrorString(e), file, line);
+    fprintf(stderr, "bbjd_gpu: %s\n", g_errbuf);
+}
+const char *last_error() { return g_errbuf; }
+
+bbjd_status Scratch::init(int64_t n_, int max_cols, int nvec) {
+    n = n_;
+    const int sms = num_sms();
+    G = (int)std::max<int64_t>(1, std::min<int64_t>(4 * sms, (n + 255) / 256));
+    rpc = ((n + G - 1) / G + 31) / 32 * 32;
+    G = (int)((n + rpc - 1) / rpc);
+    G2 = (int)std::max<int64_t>(1, std::min<int64_t>(8 * sms, (n + 255) / 256));
+    maxX = 2 * 2 * (int64_t)max_cols + 4;
+    BBJD_CUDA_TRY(cudaMalloc(&partial, sizeof(cplx) * (size_t)G * maxX));
+    BBJD_CUDA_TRY(cudaMalloc(&nrm_part, sizeof(double) * (size_t)G2));
+    BBJD_CUDA_TRY(cudaMalloc(&counter, sizeof(unsigned) * 4));
+    BBJD_CUDA_TRY(cudaMemset(counter, 0, sizeof(unsigned) * 4));
+    BBJD_CUDA_TRY(cudaMalloc(&red, sizeof(cplx) * (size_t)(nvec > 0 ? nvec : 1) * maxX));
+    BBJD_CUDA_TRY(cudaMalloc(&scal, sizeof(double) * 64));
+    BBJD_CUDA_TRY(cudaMalloc(&flags, sizeof(int) * 16));
+    BBJD_CUDA_TRY(cudaMemset(flags, 0, sizeof(int) * 16));
+    size_t smem_need = sizeof(cplx) * 2 * (size_t)rpc;
+    if (smem_need > 48 * 1024) {
+        BBJD_CUDA_TRY(cudaFuncSetAttribute(k_tsdot<1, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_need));
+        BBJD_CUDA_TRY(cudaFuncSetAttribute(k_tsdot<2, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_need));
+        BBJD_CUDA_TRY(cudaFuncSetAttribute(k_tsdot<1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_need));
+    }
+    return BBJD_SUCCESS;
+}
+
+void Scratch::release() {
+    cudaFree(partial); cudaFree(nrm_part); cudaFree(counter);
+    cudaFree(red); cudaFree(scal); cudaFree(flags);
+    partial = red = nullptr; nrm_part = scal = nullptr; counter = nullptr; flags = nullptr;
+}
+
+bbjd_status tsdot(Scratch &S, int NM, int NV, int ncols, int64_t ld, const cplx *Q0,
+                  const cplx *Q1, const cplx *v0, const cplx *v1, cplx *out, const int *flag,
+                  cudaStream_t st) {
+    const int X = NM * NV * ncols + NV;
+    if (X > S.maxX) return BBJD_ERR_INVALID;
+    const size_t smem = sizeof(cplx) * NV * (size_t)S.rpc;
+    if (NM == 1 && NV == 1)
+        k_tsdot<1, 1><<<S.G, 256, smem, st>>>(S.n, ncols, ld, Q0, Q1, v0, v1, S.rpc, S.partial, flag);
+    else if (NM == 1 && NV == 2)
+        k_tsdot<1, 2><<<S.G, 256, smem, st>>>(S.n, ncols, ld, Q0, Q1, v0, v1, S.rpc, S.partial, flag);
+    else if (NM == 2 && NV == 1)
+        k_tsdot<2, 1><<<S.G, 256, smem, st>>>(S.n, ncols, ld, Q0, Q1, v0, v1, S.rpc, S.partial, flag);
+    else
+        return BBJD_ERR_INVALID;
+    BBJD_LAUNCH_CHECK();
+    k_reduce<<<(X + 31) / 32, 256, 0, st>>>(S.partial, S.G, X, out, flag);
+    BBJD_LAUNCH_CHECK();
+    return BBJD_SUCCESS;
+}
+
+bbjd_status reduce_partials(const cplx *partial, int G, int X, cplx *out, cudaStream_t st) {
+    k_reduce<<<(X + 31) / 32, 256, 0, st>>>(partial, G, X, out, nullptr);
+    BBJD_LAUNCH_CHECK();
+    return BBJD_SUCCESS;
+}
+
+bbjd_status update(Scratch &S, int ncols, int64_t ld, const cplx *Q, const cplx *h1,
+                   const cplx *h2, cplx c1, cplx c2, cplx a, const cplx *v_in, cplx b,
+                   const cplx *w_in, cplx *v_out, double *norm_out, const cplx *ref_nsq,
+                   const double *ref_nrm, int *flag_out, const int *flag_in, cudaStream_t st) {
+    const size_t smem = sizeof(cplx) * (size_t)std::max(ncols, 1);
+    k_update<<<S.G2, 256, smem, st>>>(S.n, ncols, ld, Q, h1, h2, c1, c2, a, v_in, b, w_in, v_out,
+                                      S.nrm_part, S.counter, norm_out, ref_nsq, ref_nrm, flag_out,
+                                      flag_in);
+    BBJD_LAUNCH_CHECK();
+    return BBJD_SUCCESS;
+}
+
+bbjd_status scale_by_norm(Scratch &S, const cplx *v, const double *norm, double thresh,
+                          cplx *out, cudaStream_t st) {
+    k_scale<<<S.G2, 256, 0, st>>>(S.n, v, norm, thresh, out);
+    BBJD_LAUNCH_CHECK();
+    return BBJD_SUCCESS;
+}
+
+bbjd_status axpby(Scratch &S, const cplx *a_dev, cplx a, const cplx *x, const cplx *b_dev, cplx b,
+                  const cplx *y, cplx *out, cudaStream_t st) {
+    k_axpby<<<S.G2, 256, 0, st>>>(S.n, a_dev, a, x, b_dev, b, y, out);
+    BBJD_LAUNCH_CHECK();
+    return BBJD_SUCCESS;
+}
+
+bbjd_status svdv(Scratch &S, const cplx *dots, const cplx *z, const cplx *s, cplx *out,
+                 cudaStream_t st) {
+    k_svdv<<<S.G2, 256, 0, st>>>(S.n, dots, z, s, out);
+    BBJD_LAUNCH_CHECK();
+    return BBJD_SUCCESS;
+}
+
+bbjd_status restart_gemm(int64_t n, int k, int keep, const cplx *X, int64_t ldx, const cplx *Z_dev,
+                         int ldz, cplx *out, cudaStream_t st) {
+    const unsigned gx = (unsigned)((n + RG_ROWS - 1) / RG_ROWS);
+    // one column tile covers keep <= 16*RC; in-place needs a single tile
+    if (keep <= 16 * 2) {
+        k_restart_gemm<2><<<dim3(gx, 1), 256, 0, st>>>(n, k, keep, X, ldx, Z_dev, ldz, out);
+    } else if (keep <= 16 * 5) {
+        k_restart_gemm<5><<<dim3(gx, 1), 256, 0, st>>>(n, k, keep, X, ldx, Z_dev, ldz, out);
+    } else if (keep <= 16 * 8) {
+        k_restart_gemm<8><<<dim3(gx, 1), 256, 0, st>>>(n, k, keep, X, ldx, Z_dev, ldz, out);
+    } else {
+        if (out == X) return BBJD_ERR_INVALID;   // multi-tile form cannot run in place
+        const unsigned gy = (unsigned)((keep + 16 * 8 - 1) / (16 * 8));
+        k_restart_gemm<8><<<dim3(gx, gy), 256, 0, st>>>(n, k, keep, X, ldx, Z_dev, ldz, out);
+    }
+    BBJD_LAUNCH_CHECK();
+    return BBJD_SUCCESS;
+}
+
+bbjd_status gram(Scratch &S, int keep, const cplx *X, const cplx *Y, int64_t ldx, cplx *partial,
+                 int Gg, cplx *out, cudaStream_t st) {
+    const int64_t rpc = ((S.n + Gg - 1) / Gg + 15) / 16 * 16;
+    const unsigned gt = (unsigned)((keep + GR_T - 1) / GR_T);
+    k_gram<<<dim3((unsigned)Gg, gt, gt), 256, 0, st>>>(S.n, keep, X, Y, ldx, rpc, partial);
+    BBJD_LAUNCH_CHECK();
+    const int XX = keep * keep;
+    k_reduce<<<(XX + 31) / 32, 256, 0, st>>>(partial, Gg, XX, out, nullptr);
+    BBJD_LAUNCH_CHECK();
+    return BBJD_SUCCESS;
+}
+
+}  // namespace bbjd

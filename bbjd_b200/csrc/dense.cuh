@@ -1,0 +1,56 @@
+// Host-side interface of the tall-skinny dense kernels (dense.cu).
+#pragma once
+
+#include "common.cuh"
+
+namespace bbjd {
+
+const char *last_error();
+
+// Per-solve scratch for two-stage reductions.  One Scratch per stream:
+// the last-CTA norm counter is not shared between concurrent launches.
+struct Scratch {
+    int64_t n = 0;
+    int G = 0;          // CTAs of the dot kernels
+    int64_t rpc = 0;    // rows per dot CTA
+    int G2 = 0;         // CTAs of the streaming update kernels
+    int64_t maxX = 0;
+    cplx *partial = nullptr;
+    double *nrm_part = nullptr;
+    unsigned *counter = nullptr;
+    cplx *red = nullptr;     // reduced dot outputs
+    double *scal = nullptr;  // device scalar slots
+    int *flags = nullptr;    // device flags
+    bbjd_status init(int64_t n, int max_cols, int nvec);
+    void release();
+};
+
+// out[x] = sum over rows of conj(Q_m[:, j]) v_p, x = (m*NV + p)*ncols + j;
+// out[NM*NV*ncols + p] = ||v_p||^2.  Skipped when flag && *flag == 0.
+bbjd_status tsdot(Scratch &S, int NM, int NV, int ncols, int64_t ld, const cplx *Q0,
+                  const cplx *Q1, const cplx *v0, const cplx *v1, cplx *out, const int *flag,
+                  cudaStream_t st);
+
+// v_out = a v_in + b w_in - Q (c1 h1 + c2 h2); *norm_out = ||v_out||;
+// *flag_out = ||v_out|| < 0.7071 ||v_before|| with ||v_before|| = sqrt(ref_nsq.x)
+// or *ref_nrm.  Skipped when flag_in && !*flag_in.  Q may be null when ncols == 0.
+bbjd_status update(Scratch &S, int ncols, int64_t ld, const cplx *Q, const cplx *h1,
+                   const cplx *h2, cplx c1, cplx c2, cplx a, const cplx *v_in, cplx b,
+                   const cplx *w_in, cplx *v_out, double *norm_out, const cplx *ref_nsq,
+                   const double *ref_nrm, int *flag_out, const int *flag_in, cudaStream_t st);
+
+bbjd_status scale_by_norm(Scratch &S, const cplx *v, const double *norm, double thresh,
+                          cplx *out, cudaStream_t st);
+bbjd_status axpby(Scratch &S, const cplx *a_dev, cplx a, const cplx *x, const cplx *b_dev, cplx b,
+                  const cplx *y, cplx *out, cudaStream_t st);
+bbjd_status svdv(Scratch &S, const cplx *dots, const cplx *z, const cplx *s, cplx *out,
+                 cudaStream_t st);
+bbjd_status restart_gemm(int64_t n, int k, int keep, const cplx *X, int64_t ldx, const cplx *Z_dev,
+                         int ldz, cplx *out, cudaStream_t st);
+// out[x] = sum_g partial[g*X + x], fixed order.
+bbjd_status reduce_partials(const cplx *partial, int G, int X, cplx *out, cudaStream_t st);
+// out (keep x keep col-major, device) = X^H Y; partial holds Gg*keep*keep.
+bbjd_status gram(Scratch &S, int keep, const cplx *X, const cplx *Y, int64_t ldx, cplx *partial,
+                 int Gg, cplx *out, cudaStream_t st);
+
+}  // namespace bbjd

@@ -1,0 +1,109 @@
+// The JDQZ engine: host driver state shared by the device-operator and the
+// host-callback entry points.
+#pragma once
+
+#include <chrono>
+#include <complex>
+#include <vector>
+
+#include "bbt.cuh"
+
+namespace bbjd {
+
+typedef std::complex<double> zc;
+
+// Operators of one solve: A and B products (with the optional fused
+// residual r = tb A x - ta B x and its norm) and the preconditioner.
+struct Operators {
+    virtual ~Operators() {}
+    // yA = A x, yB = B x; if r: r = tb yA - ta yB and *rnorm_dev = ||r||.
+    virtual bbjd_status apply(const cplx *x, cplx *yA, cplx *yB, cplx ta, cplx tb, cplx *r,
+                              double *rnorm_dev) = 0;
+    virtual bool has_precond() const = 0;
+    // x[:, q] = M^-1 r[:, q] for q < nrhs (stride n).
+    virtual bbjd_status precond(int nrhs, const cplx *r, cplx *x) = 0;
+    virtual double apply_bytes(bool residual) const = 0;
+    virtual double precond_bytes(int nrhs) const = 0;
+};
+
+Operators *make_device_ops(const bbjd_bbt_matrix *m, const bbjd_precond *pc, Scratch *S,
+                           cudaStream_t st);
+Operators *make_callback_ops(const bbjd_params *p, Scratch *S, cudaStream_t st, int *cb_failed);
+
+enum KClass { KC_SPMV = 0, KC_ORTH, KC_PENCIL, KC_RITZ, KC_PRECOND, KC_RESTART, KC_SMALL, KC_GMRES, KC_N };
+
+// Device timing of kernel classes with CUDA events on the solve's stream.
+struct Timer {
+    bool on = false;
+    cudaStream_t st = nullptr;
+    struct Rec { int cls; cudaEvent_t a, b; double bytes; };
+    std::vector<Rec> pending;
+    std::vector<cudaEvent_t> pool;
+    double ms[KC_N] = {0}, bytes[KC_N] = {0};
+    long long calls[KC_N] = {0};
+    int cur_cls = -1;
+    cudaEvent_t cur_a = nullptr;
+    double cur_bytes = 0;
+    cudaEvent_t get();
+    void begin(int cls, double b);
+    void end();
+    void flush();   // after a stream sync
+    void release();
+};
+
+struct Engine {
+    const bbjd_params *P = nullptr;
+    bbjd_workspace *ws = nullptr;
+    bbjd_result *res = nullptr;
+    bbjd_device_ext *ext = nullptr;
+    Operators *ops = nullptr;
+    Scratch S;
+    cudaStream_t st = nullptr;
+    bool own_stream = false;
+    Timer T;
+
+    int64_t n = 0, maxsub = 0, nev = 0, minsub = 0;
+    zc sigma, nu0, mu0;
+    int target = 0;
+    double tol = 0;
+
+    // device buffers owned by the engine
+    cplx *ru = nullptr;    // [r | u]  (2n)
+    cplx *zs = nullptr;    // [z | s]  (2n)
+    cplx *Au = nullptr, *Bu = nullptr;
+    cplx *g1 = nullptr, *g2 = nullptr, *g3 = nullptr;  // GMRES / scratch vectors
+    cplx *Zdev = nullptr;  // maxsub x maxsub restart coefficients
+    cplx *xdev = nullptr;  // maxsub Ritz / combination coefficients
+    cplx *gram_part = nullptr;
+    int gram_G = 0;
+    cplx *gram_out = nullptr;  // 2 x maxsub^2
+    double *dscal = nullptr;   // device scalars
+    int *dflag = nullptr;      // device flags
+    cplx *pin = nullptr;       // pinned host staging for small results
+    double *pin_d = nullptr;
+    int *pin_i = nullptr;
+
+    // host LAPACK workspace of the projected solve
+    std::vector<zc> alpha, beta, zwork;
+    std::vector<double> rwork;
+    std::vector<int> bwork, sel, iwork;
+    double qz_seconds = 0;
+    long long dgks = 0, restarts = 0;
+    double bytes_dev = 0;
+
+    bbjd_status init(const bbjd_params *p, bbjd_workspace *w, bbjd_result *r, bbjd_device_ext *e,
+                     Operators *o, cudaStream_t stream);
+    void release();
+    bbjd_status run();
+
+    // building blocks
+    bbjd_status orthogonalize(const cplx *Q, int64_t ldq, int k, cplx *v, double *norm_dev,
+                              int cls);
+    bbjd_status project_out(const cplx *Q, int k, cplx *v, int cls);
+    bbjd_status deflation_append(int j, const cplx *u, const cplx *Au_, const cplx *Bu_);
+    bbjd_status gmres(int ndefl, zc ta, zc tb, const cplx *r, cplx *z);
+    int solve_projected(int k, int locked, int nkeep, int *target_pos);
+    bbjd_status sync();
+};
+
+}  // namespace bbjd

@@ -1,0 +1,755 @@
+// JDQZ outer iteration on one GPU (restates reference src/jd_core.c:743-1120
+// as a host driver over device kernels).
+//
+// Per iteration only k x k data crosses PCIe: the projected pencil's new
+// row and column (device -> host), the Ritz coefficients and, at a restart,
+// the kept Schur vectors (host -> device).  Every n-sized vector and the
+// search / test spaces stay in HBM.  The projected QZ, reordering, target
+// scan and Givens rotations run in FP64 on the host through LAPACK (ZGGES,
+// ZTGSEN), exactly as the reference calls them.
+#include "engine.cuh"
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <cfloat>
+
+extern "C" {
+void scipy_zgges_(const char *jobvsl, const char *jobvsr, const char *sort, void *selctg,
+                  const int *n, bbjd_zomplex *a, const int *lda, bbjd_zomplex *b, const int *ldb,
+                  int *sdim, bbjd_zomplex *alpha, bbjd_zomplex *beta, bbjd_zomplex *vsl,
+                  const int *ldvsl, bbjd_zomplex *vsr, const int *ldvsr, bbjd_zomplex *work,
+                  const int *lwork, double *rwork, int *bwork, int *info);
+void scipy_ztgsen_(const int *ijob, const int *wantq, const int *wantz, const int *select,
+                   const int *n, bbjd_zomplex *a, const int *lda, bbjd_zomplex *b, const int *ldb,
+                   bbjd_zomplex *alpha, bbjd_zomplex *beta, bbjd_zomplex *q, const int *ldq,
+                   bbjd_zomplex *z, const int *ldz, int *m, double *pl, double *pr, double *dif,
+                   bbjd_zomplex *work, const int *lwork, int *iwork, const int *liwork, int *info);
+}
+
+namespace bbjd {
+
+static inline cplx C(zc z) { return mk(z.real(), z.imag()); }
+static inline zc Z(cplx c) { return zc(c.x, c.y); }
+
+// device scalar slots
+enum { SC_UNORM = 0, SC_RNORM, SC_VNORM, SC_WNORM, SC_TMP, SC_TMP2, SC_GNORM, SC_WPRE, SC_N };
+// device flag slots
+enum { FL_V = 0, FL_W, FL_T, FL_G, FL_N };
+
+// ---------------------------------------------------------------------------
+cudaEvent_t Timer::get() {
+    if (!pool.empty()) {
+        cudaEvent_t e = pool.back();
+        pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    return e;
+}
+void Timer::begin(int cls, double b) {
+    if (!on) { bytes[cls] += b; calls[cls]++; return; }
+    cur_cls = cls;
+    cur_bytes = b;
+    cur_a = get();
+    cudaEventRecord(cur_a, st);
+}
+void Timer::end() {
+    if (!on || cur_cls < 0) return;
+    cudaEvent_t b = get();
+    cudaEventRecord(b, st);
+    pending.push_back({cur_cls, cur_a, b, cur_bytes});
+    cur_cls = -1;
+}
+void Timer::flush() {
+    for (auto &r : pending) {
+        float t = 0.f;
+        cudaEventElapsedTime(&t, r.a, r.b);
+        ms[r.cls] += t;
+        bytes[r.cls] += r.bytes;
+        calls[r.cls]++;
+        pool.push_back(r.a);
+        pool.push_back(r.b);
+    }
+    pending.clear();
+}
+void Timer::release() {
+    flush();
+    for (auto e : pool) cudaEventDestroy(e);
+    pool.clear();
+}
+
+// ---------------------------------------------------------------------------
+bbjd_status Engine::init(const bbjd_params *p, bbjd_workspace *w, bbjd_result *r,
+                         bbjd_device_ext *e, Operators *o, cudaStream_t stream) {
+    P = p;
+    ws = w;
+    res = r;
+    ext = e;
+    ops = o;
+    n = p->n;
+    nev = p->nev;
+    maxsub = w->maxsub;
+    const int64_t minsub_auto = std::max<int64_t>(2 * nev + 5, 20);    // jd_core.c:750-752
+    minsub = p->minsub > 0 ? p->minsub : minsub_auto;
+    sigma = p->sigma;
+    target = (int)p->target;
+    tol = p->tol;
+    if (stream) {
+        st = stream;
+    } else {
+        BBJD_CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        own_stream = true;
+    }
+    T.on = e && e->record_timing;
+    T.st = st;
+    bbjd_status s = S.init(n, (int)(maxsub + nev + 2), 4);
+    if (s != BBJD_SUCCESS) return s;
+    const size_t nv = sizeof(cplx) * (size_t)n;
+    BBJD_CUDA_TRY(cudaMalloc(&ru, 2 * nv));
+    BBJD_CUDA_TRY(cudaMalloc(&zs, 2 * nv));
+    BBJD_CUDA_TRY(cudaMalloc(&Au, nv));
+    BBJD_CUDA_TRY(cudaMalloc(&Bu, nv));
+    BBJD_CUDA_TRY(cudaMalloc(&g1, nv));
+    BBJD_CUDA_TRY(cudaMalloc(&g2, nv));
+    BBJD_CUDA_TRY(cudaMalloc(&g3, nv));
+    BBJD_CUDA_TRY(cudaMalloc(&Zdev, sizeof(cplx) * maxsub * maxsub));
+    BBJD_CUDA_TRY(cudaMalloc(&xdev, sizeof(cplx) * (2 * maxsub + nev + 8)));
+    gram_G = (int)std::max<int64_t>(1, std::min<int64_t>(num_sms(), (n + 1023) / 1024));
+    BBJD_CUDA_TRY(cudaMalloc(&gram_part, sizeof(cplx) * (size_t)gram_G * maxsub * maxsub));
+    BBJD_CUDA_TRY(cudaMalloc(&gram_out, sizeof(cplx) * 2 * maxsub * maxsub));
+    BBJD_CUDA_TRY(cudaMalloc(&dscal, sizeof(double) * SC_N));
+    BBJD_CUDA_TRY(cudaMalloc(&dflag, sizeof(int) * FL_N));
+    BBJD_CUDA_TRY(cudaMemset(dflag, 0, sizeof(int) * FL_N));
+    const size_t pin_c = 8 * (size_t)(maxsub + nev + 8);
+    BBJD_CUDA_TRY(cudaMallocHost(&pin, sizeof(cplx) * pin_c));
+    BBJD_CUDA_TRY(cudaMallocHost(&pin_d, sizeof(double) * 16));
+    BBJD_CUDA_TRY(cudaMallocHost(&pin_i, sizeof(int) * 16));
+    alpha.resize(maxsub);
+    beta.resize(maxsub);
+    rwork.resize(8 * maxsub);
+    bwork.resize(maxsub);
+    sel.resize(maxsub);
+    return BBJD_SUCCESS;
+}
+
+void Engine::release() {
+    T.release();
+    S.release();
+    cudaFree(ru); cudaFree(zs); cudaFree(Au); cudaFree(Bu);
+    cudaFree(g1); cudaFree(g2); cudaFree(g3);
+    cudaFree(Zdev); cudaFree(xdev); cudaFree(gram_part); cudaFree(gram_out);
+    cudaFree(dscal); cudaFree(dflag);
+    cudaFreeHost(pin); cudaFreeHost(pin_d); cudaFreeHost(pin_i);
+    if (own_stream && st) cudaStreamDestroy(st);
+    st = nullptr;
+}
+
+bbjd_status Engine::sync() {
+    BBJD_CUDA_TRY(cudaStreamSynchronize(st));
+    T.flush();
+    return BBJD_SUCCESS;
+}
+
+// CGS with a DGKS re-pass of v against Q[:, 0:k] (reference jd_core.c:207-241);
+// the final norm lands in *norm_dev.  The re-pass decision is taken on the
+// device (flag), so no host round trip is needed.
+bbjd_status Engine::orthogonalize(const cplx *Q, int64_t ldq, int k, cplx *v, double *norm_dev,
+                                  int cls) {
+    bbjd_status s;
+    const double pass_bytes = 16.0 * (double)n * (2.0 * k + 3.0);
+    T.begin(cls, pass_bytes);
+    if (k == 0) {
+        s = update(S, 0, ldq, nullptr, nullptr, nullptr, mk(0, 0), mk(0, 0), mk(1, 0), v, mk(0, 0),
+                   nullptr, v, norm_dev, nullptr, nullptr, nullptr, nullptr, st);
+        T.end();
+        bytes_dev += 32.0 * n;
+        return s;
+    }
+    int *flag = dflag + FL_T;
+    cplx *h = S.red;
+    s = tsdot(S, 1, 1, k, ldq, Q, nullptr, v, nullptr, h, nullptr, st);
+    if (s) return s;
+    s = update(S, k, ldq, Q, h, nullptr, mk(1, 0), mk(0, 0), mk(1, 0), v, mk(0, 0), nullptr, v,
+               norm_dev, h + k, nullptr, flag, nullptr, st);
+    if (s) return s;
+    // second pass, executed only when the device raised the DGKS flag
+    cplx *h2 = S.red + S.maxX;
+    s = tsdot(S, 1, 1, k, ldq, Q, nullptr, v, nullptr, h2, flag, st);
+    if (s) return s;
+    s = update(S, k, ldq, Q, h2, nullptr, mk(1, 0), mk(0, 0), mk(1, 0), v, mk(0, 0), nullptr, v,
+               norm_dev, nullptr, nullptr, nullptr, flag, st);
+    T.end();
+    bytes_dev += pass_bytes;
+    return s;
+}
+
+// Two unconditional CGS passes (reference jd_core.c:269-309).
+bbjd_status Engine::project_out(const cplx *Q, int k, cplx *v, int cls) {
+    if (k == 0) return BBJD_SUCCESS;
+    for (int pass = 0; pass < 2; ++pass) {
+        T.begin(cls, 16.0 * n * (2.0 * k + 3.0));
+        bbjd_status s = tsdot(S, 1, 1, k, n, Q, nullptr, v, nullptr, S.red, nullptr, st);
+        if (s) return s;
+        s = update(S, k, n, Q, S.red, nullptr, mk(1, 0), mk(0, 0), mk(1, 0), v, mk(0, 0), nullptr,
+                   v, dscal + SC_TMP, nullptr, nullptr, nullptr, nullptr, st);
+        if (s) return s;
+        T.end();
+        bytes_dev += 16.0 * n * (2.0 * k + 3.0);
+    }
+    return BBJD_SUCCESS;
+}
+
+// Column j of the deflation projectors (reference jd_core.c:516-528).
+bbjd_status Engine::deflation_append(int j, const cplx *u, const cplx *Au_, const cplx *Bu_) {
+    cplx *qr = reinterpret_cast<cplx *>(ws->Q_right) + (int64_t)j * n;
+    cplx *ql = reinterpret_cast<cplx *>(ws->Q_left) + (int64_t)j * n;
+    BBJD_CUDA_TRY(cudaMemcpyAsync(qr, u, sizeof(cplx) * n, cudaMemcpyDeviceToDevice, st));
+    bbjd_status s = orthogonalize(reinterpret_cast<cplx *>(ws->Q_right), n, j, qr, dscal + SC_TMP, KC_SMALL);
+    if (s) return s;
+    s = scale_by_norm(S, qr, dscal + SC_TMP, 1e-300, qr, st);
+    if (s) return s;
+    s = axpby(S, nullptr, C(nu0), Au_, nullptr, C(mu0), Bu_, ql, st);
+    if (s) return s;
+    s = orthogonalize(reinterpret_cast<cplx *>(ws->Q_left), n, j, ql, dscal + SC_TMP, KC_SMALL);
+    if (s) return s;
+    return scale_by_norm(S, ql, dscal + SC_TMP, 1e-300, ql, st);
+}
+
+// ---------------------------------------------------------------------------
+// Selection key of reference jd_core.c:387-396 (smaller is better).
+static double target_value(zc lam, zc sigma, int target) {
+    switch (target) {
+        case BBJD_TARGET_NEAREST: return std::abs(lam - sigma);
+        case BBJD_TARGET_LARGEST_MAG: return -std::abs(lam);
+        case BBJD_TARGET_SMALLEST_MAG: return std::abs(lam);
+        case BBJD_TARGET_LARGEST_REAL: return -lam.real();
+        case BBJD_TARGET_SMALLEST_REAL: return lam.real();
+        case BBJD_TARGET_LARGEST_IMAG: return -lam.imag();
+        case BBJD_TARGET_SMALLEST_IMAG: return lam.imag();
+        default: return std::abs(lam - sigma);
+    }
+}
+
+// ZGGES + SELECT + ZTGSEN + target scan (reference jd_core.c:319-462), on the
+// workspace's host MA, MB (ld = maxsub).  Returns 0 or -1 on a LAPACK error.
+int Engine::solve_projected(int k, int locked, int nkeep, int *target_pos) {
+    (void)locked;
+    auto t0 = std::chrono::steady_clock::now();
+    const int bk = k, lda = (int)maxsub;
+    zc *MA = ws->MA, *MB = ws->MB, *SA = ws->SA, *SB = ws->SB, *ZA = ws->ZA, *ZB = ws->ZB;
+    for (int j = 0; j < k; ++j) {
+        memcpy(SA + (size_t)j * maxsub, MA + (size_t)j * maxsub, sizeof(zc) * k);
+        memcpy(SB + (size_t)j * maxsub, MB + (size_t)j * maxsub, sizeof(zc) * k);
+    }
+    int sdim = 0, info = 0, lwork = -1;
+    zc wq;
+    scipy_zgges_("V", "V", "N", nullptr, &bk, SA, &lda, SB, &lda, &sdim, alpha.data(), beta.data(),
+                 ZA, &lda, ZB, &lda, &wq, &lwork, rwork.data(), bwork.data(), &info);
+    if (info) return -1;
+    lwork = (int)wq.real() + 1;
+    if ((int)zwork.size() < lwork) zwork.resize(lwork);
+    scipy_zgges_("V", "V", "N", nullptr, &bk, SA, &lda, SB, &lda, &sdim, alpha.data(), beta.data(),
+                 ZA, &lda, ZB, &lda, zwork.data(), &lwork, rwork.data(), bwork.data(), &info);
+    if (info) return -1;
+    const zc *conv = res->eigenvalues;
+    const int64_t nconv = res->nconv;
+    std::fill(sel.begin(), sel.begin() + k, 0);
+    for (int i = 0; i < k; ++i) {                                   // jd_core.c:365-374
+        if (std::abs(beta[i]) < 1e-300) continue;
+        const zc lam = alpha[i] / beta[i];
+        for (int64_t c = 0; c < nconv; ++c)
+            if (std::abs(lam - conv[c]) < tol * 100) { sel[i] = 1; break; }
+    }
+    for (int pick = 0; pick < nkeep; ++pick) {                      // jd_core.c:379-401
+        int tidx = -1;
+        double best = DBL_MAX;
+        for (int i = 0; i < k; ++i) {
+            if (sel[i] || std::abs(beta[i]) < 1e-300) continue;
+            const double v = target_value(alpha[i] / beta[i], sigma, target);
+            if (v < best) { best = v; tidx = i; }
+        }
+        if (tidx < 0) break;
+        sel[tidx] = 1;
+    }
+    int nsel = 0;
+    for (int i = 0; i < k; ++i) nsel += sel[i];
+    if (nsel > 0) {                                                 // jd_core.c:407-425
+        int m_out = 0, wantq = 1, wantz = 1, ijob = 0, tlw = -1, tli = -1, tiq = 0;
+        double pl, pr, dif[2];
+        zc twq;
+        scipy_ztgsen_(&ijob, &wantq, &wantz, sel.data(), &bk, SA, &lda, SB, &lda, alpha.data(),
+                      beta.data(), ZA, &lda, ZB, &lda, &m_out, &pl, &pr, dif, &twq, &tlw, &tiq,
+                      &tli, &info);
+        tlw = (int)twq.real() + 1;
+        tli = tiq + 1;
+        if ((int)zwork.size() < tlw) zwork.resize(tlw);
+        if ((int)iwork.size() < tli) iwork.resize(tli);
+        scipy_ztgsen_(&ijob, &wantq, &wantz, sel.data(), &bk, SA, &lda, SB, &lda, alpha.data(),
+                      beta.data(), ZA, &lda, ZB, &lda, &m_out, &pl, &pr, dif, zwork.data(), &tlw,
+                      iwork.data(), &tli, &info);
+        if (info) return -1;
+    }
+    int tpos = 0;                                                   // jd_core.c:430-458
+    double best = DBL_MAX;
+    for (int i = 0; i < k; ++i) {
+        if (std::abs(beta[i]) < 1e-300) continue;
+        const zc lam = alpha[i] / beta[i];
+        bool is_conv = false;
+        for (int64_t c = 0; c < nconv; ++c)
+            if (std::abs(lam - conv[c]) < tol * 100) { is_conv = true; break; }
+        if (is_conv) continue;
+        const double v = target_value(lam, sigma, target);
+        if (v < best) { best = v; tpos = i; }
+    }
+    *target_pos = tpos;
+    qz_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return 0;
+}
+
+// Complex Givens with real cs >= 0 (reference jd_core.c:477-511).
+static void zlartg_stable(zc f, zc g, double *cs, zc *sn, zc *r) {
+    const double af = std::abs(f), ag = std::abs(g);
+    if (ag < 1e-300) { *cs = 1.0; *sn = 0.0; *r = f; return; }
+    if (af < 1e-300) { *cs = 0.0; *sn = std::conj(g) / ag; *r = ag; return; }
+    const double scale = af + ag, fs = af / scale, gs = ag / scale;
+    const double norm = scale * std::sqrt(fs * fs + gs * gs);
+    *cs = af / norm;
+    *sn = (f / af) * std::conj(g) / norm;
+    *r = (f / af) * norm;
+}
+
+// Left-preconditioned GMRES on the projected correction equation
+// (reference jd_core.c:568-727).  The Arnoldi step orthogonalises with CGS
+// plus the same DGKS re-pass test instead of the reference's MGS loop: the
+// same H column in exact arithmetic, two streaming passes over the basis
+// instead of 2(j+1) dependent BLAS-1 calls.
+bbjd_status Engine::gmres(int ndefl, zc ta, zc tb, const cplx *r, cplx *z) {
+    const int ims = (int)P->inner_maxiter;
+    cplx *V = reinterpret_cast<cplx *>(ws->gmres_V);
+    const cplx *Qr = reinterpret_cast<cplx *>(ws->Q_right);
+    const cplx *Ql = reinterpret_cast<cplx *>(ws->Q_left);
+    zc *H = ws->gmres_H, *sn = ws->gmres_sn, *g = ws->gmres_g;
+    double *cs = reinterpret_cast<double *>(ws->gmres_cs);
+    const double itol = P->inner_tol;
+    std::fill(H, H + (size_t)(ims + 1) * ims, zc(0));
+    bbjd_status s;
+    // v0 = -M^-1 P_L r
+    s = axpby(S, nullptr, mk(-1, 0), r, nullptr, mk(0, 0), nullptr, g1, st);
+    if (s) return s;
+    s = project_out(Ql, ndefl, g1, KC_GMRES);
+    if (s) return s;
+    if (ops->has_precond()) {
+        T.begin(KC_PRECOND, ops->precond_bytes(1));
+        s = ops->precond(1, g1, V);
+        T.end();
+        bytes_dev += ops->precond_bytes(1);
+    } else {
+        s = cudaMemcpyAsync(V, g1, sizeof(cplx) * n, cudaMemcpyDeviceToDevice, st) ? BBJD_ERR_CUDA : BBJD_SUCCESS;
+    }
+    if (s) return s;
+    s = update(S, 0, n, nullptr, nullptr, nullptr, mk(0, 0), mk(0, 0), mk(1, 0), V, mk(0, 0), nullptr,
+               V, dscal + SC_GNORM, nullptr, nullptr, nullptr, nullptr, st);
+    if (s) return s;
+    BBJD_CUDA_TRY(cudaMemcpyAsync(pin_d, dscal + SC_GNORM, sizeof(double), cudaMemcpyDeviceToHost, st));
+    if ((s = sync())) return s;
+    const double beta0 = pin_d[0];
+    if (beta0 < 1e-300) {
+        BBJD_CUDA_TRY(cudaMemsetAsync(z, 0, sizeof(cplx) * n, st));
+        return BBJD_SUCCESS;
+    }
+    s = scale_by_norm(S, V, dscal + SC_GNORM, 0.0, V, st);
+    if (s) return s;
+    std::fill(g, g + ims + 1, zc(0));
+    g[0] = beta0;
+    int j;
+    for (j = 0; j < ims; ++j) {
+        cplx *vj = V + (int64_t)j * n, *vj1 = V + (int64_t)(j + 1) * n;
+        BBJD_CUDA_TRY(cudaMemcpyAsync(g1, vj, sizeof(cplx) * n, cudaMemcpyDeviceToDevice, st));
+        if ((s = project_out(Qr, ndefl, g1, KC_GMRES))) return s;
+        T.begin(KC_SPMV, ops->apply_bytes(true));
+        s = ops->apply(g1, g2, g3, C(ta), C(tb), vj1, dscal + SC_TMP2);   // vj1 = tb A g1 - ta B g1
+        T.end();
+        bytes_dev += ops->apply_bytes(true);
+        if (s) return s;
+        if ((s = project_out(Ql, ndefl, vj1, KC_GMRES))) return s;
+        if (ops->has_precond()) {
+            BBJD_CUDA_TRY(cudaMemcpyAsync(g2, vj1, sizeof(cplx) * n, cudaMemcpyDeviceToDevice, st));
+            T.begin(KC_PRECOND, ops->precond_bytes(1));
+            s = ops->precond(1, g2, vj1);
+            T.end();
+            bytes_dev += ops->precond_bytes(1);
+            if (s) return s;
+        }
+        // Arnoldi: CGS + DGKS against V[:, 0:j+1]; H column from both passes
+        const int kk = j + 1;
+        int *flag = dflag + FL_G;
+        T.begin(KC_GMRES, 16.0 * n * (2.0 * kk + 3.0));
+        if ((s = tsdot(S, 1, 1, kk, n, V, nullptr, vj1, nullptr, S.red, nullptr, st))) return s;
+        if ((s = update(S, kk, n, V, S.red, nullptr, mk(1, 0), mk(0, 0), mk(1, 0), vj1, mk(0, 0), nullptr,
+                        vj1, dscal + SC_GNORM, S.red + kk, nullptr, flag, nullptr, st)))
+            return s;
+        cplx *h2 = S.red + S.maxX;
+        BBJD_CUDA_TRY(cudaMemsetAsync(h2, 0, sizeof(cplx) * kk, st));
+        if ((s = tsdot(S, 1, 1, kk, n, V, nullptr, vj1, nullptr, h2, flag, st))) return s;
+        if ((s = update(S, kk, n, V, h2, nullptr, mk(1, 0), mk(0, 0), mk(1, 0), vj1, mk(0, 0), nullptr,
+                        vj1, dscal + SC_GNORM, nullptr, nullptr, nullptr, flag, st)))
+            return s;
+        T.end();
+        bytes_dev += 16.0 * n * (2.0 * kk + 3.0);
+        BBJD_CUDA_TRY(cudaMemcpyAsync(pin, S.red, sizeof(cplx) * (kk + 1), cudaMemcpyDeviceToHost, st));
+        BBJD_CUDA_TRY(cudaMemcpyAsync(pin + kk + 1, h2, sizeof(cplx) * kk, cudaMemcpyDeviceToHost, st));
+        BBJD_CUDA_TRY(cudaMemcpyAsync(pin_d, dscal + SC_GNORM, sizeof(double), cudaMemcpyDeviceToHost, st));
+        BBJD_CUDA_TRY(cudaMemcpyAsync(pin_i, flag, sizeof(int), cudaMemcpyDeviceToHost, st));
+        if ((s = sync())) return s;
+        const double w_before = std::sqrt(pin[kk].x);
+        for (int i = 0; i < kk; ++i) {
+            zc h = Z(pin[i]);
+            if (pin_i[0]) h += Z(pin[kk + 1 + i]);
+            H[i + (size_t)j * (ims + 1)] = h;
+        }
+        if (pin_i[0]) dgks++;
+        const double hjj1 = pin_d[0];
+        H[(j + 1) + (size_t)j * (ims + 1)] = hjj1;
+        if (hjj1 < 1e-14 * w_before) { j++; break; }               // jd_core.c:674
+        if ((s = scale_by_norm(S, vj1, dscal + SC_GNORM, 0.0, vj1, st))) return s;
+        for (int i = 0; i < j; ++i) {                               // jd_core.c:680-685
+            const zc h1 = H[i + (size_t)j * (ims + 1)], h2v = H[i + 1 + (size_t)j * (ims + 1)];
+            H[i + (size_t)j * (ims + 1)] = cs[i] * h1 + sn[i] * h2v;
+            H[i + 1 + (size_t)j * (ims + 1)] = -std::conj(sn[i]) * h1 + cs[i] * h2v;
+        }
+        double csj;
+        zc snj, rj;
+        zlartg_stable(H[j + (size_t)j * (ims + 1)], H[(j + 1) + (size_t)j * (ims + 1)], &csj, &snj, &rj);
+        cs[j] = csj;
+        sn[j] = snj;
+        H[j + (size_t)j * (ims + 1)] = rj;
+        H[j + 1 + (size_t)j * (ims + 1)] = 0.0;
+        const zc ga = g[j], gb = g[j + 1];
+        g[j] = cs[j] * ga + sn[j] * gb;
+        g[j + 1] = -std::conj(sn[j]) * ga + cs[j] * gb;
+        if (std::abs(g[j + 1]) < itol * beta0) { j++; break; }      // jd_core.c:705
+    }
+    const int m = j;
+    zc *y = g;                                                      // jd_core.c:711-716
+    for (int i = m - 1; i >= 0; --i) {
+        for (int k2 = i + 1; k2 < m; ++k2) y[i] -= H[i + (size_t)k2 * (ims + 1)] * y[k2];
+        if (std::abs(H[i + (size_t)i * (ims + 1)]) > 1e-300) y[i] /= H[i + (size_t)i * (ims + 1)];
+    }
+    // z = V_m y  (update with c1 = -1 computes 0 - V(-y))
+    for (int i = 0; i < m; ++i) pin[i] = C(y[i]);
+    BBJD_CUDA_TRY(cudaMemcpyAsync(xdev, pin, sizeof(cplx) * std::max(m, 1), cudaMemcpyHostToDevice, st));
+    T.begin(KC_GMRES, 16.0 * n * (m + 1.0));
+    if ((s = update(S, m, n, V, xdev, nullptr, mk(-1, 0), mk(0, 0), mk(0, 0), nullptr, mk(0, 0), nullptr, z,
+                    dscal + SC_TMP, nullptr, nullptr, nullptr, nullptr, st)))
+        return s;
+    T.end();
+    bytes_dev += 16.0 * n * (m + 1.0);
+    return project_out(Qr, ndefl, z, KC_GMRES);                     // jd_core.c:724
+}
+
+// ---------------------------------------------------------------------------
+bbjd_status Engine::run() {
+    bbjd_status s;
+    const int64_t ld = n;
+    cplx *V = reinterpret_cast<cplx *>(ws->V), *W = reinterpret_cast<cplx *>(ws->W);
+    cplx *AV = reinterpret_cast<cplx *>(ws->AV), *BV = reinterpret_cast<cplx *>(ws->BV);
+    cplx *r = ru, *u = ru + n, *z = zs, *sv = zs + n;
+    const double abytes_r = ops->apply_bytes(true), abytes = ops->apply_bytes(false);
+
+    res->nconv = 0;
+    res->iters = 0;
+    res->status = BBJD_SUCCESS;
+
+    nu0 = 0.0;                                                      // jd_core.c:783-789
+    mu0 = 1.0;
+    if (target == BBJD_TARGET_NEAREST) {
+        const double sc = 1.0 / std::sqrt(1.0 + std::abs(sigma) * std::abs(sigma));
+        nu0 = sc;
+        mu0 = -sigma * sc;
+    } else if (target == BBJD_TARGET_SMALLEST_MAG) {
+        nu0 = 1.0;
+        mu0 = 0.0;
+    }
+    // start vector (jd_core.c:791-805): v0, else the C library's rand() seeded 42
+    ws->kdim = 0;
+    ws->nlock = 0;
+    srand(42);
+    {
+        std::vector<zc> v0h;
+        const zc *src = P->v0;
+        if (!src) {
+            v0h.resize(n);
+            for (int64_t i = 0; i < n; ++i) {
+                const double re = (double)rand() / RAND_MAX - 0.5;
+                const double im = (double)rand() / RAND_MAX - 0.5;
+                v0h[i] = zc(re, im);
+            }
+            src = v0h.data();
+        }
+        BBJD_CUDA_TRY(cudaMemcpyAsync(V, src, sizeof(cplx) * n, cudaMemcpyHostToDevice, st));
+        if ((s = update(S, 0, ld, nullptr, nullptr, nullptr, mk(0, 0), mk(0, 0), mk(1, 0), V, mk(0, 0),
+                        nullptr, V, dscal + SC_VNORM, nullptr, nullptr, nullptr, nullptr, st)))
+            return s;
+        BBJD_CUDA_TRY(cudaMemcpyAsync(pin_d, dscal + SC_VNORM, sizeof(double), cudaMemcpyDeviceToHost, st));
+        if ((s = sync())) return s;
+    }
+    if (pin_d[0] < 1e-300) return res->status = BBJD_ERR_BREAKDOWN;
+    if ((s = scale_by_norm(S, V, dscal + SC_VNORM, 0.0, V, st))) return s;
+    T.begin(KC_SPMV, abytes);
+    s = ops->apply(V, AV, BV, mk(0, 0), mk(0, 0), nullptr, nullptr);  // jd_core.c:807-810
+    T.end();
+    bytes_dev += abytes;
+    if (s) return s;
+    // W0 = (nu0 AV0 + mu0 BV0) / || . ||  (jd_core.c:812-816)
+    if ((s = update(S, 0, ld, nullptr, nullptr, nullptr, mk(0, 0), mk(0, 0), C(nu0), AV, C(mu0), BV, W,
+                    dscal + SC_WNORM, nullptr, nullptr, nullptr, nullptr, st)))
+        return s;
+    if ((s = scale_by_norm(S, W, dscal + SC_WNORM, 0.0, W, st))) return s;
+    // MA0 = W0^H AV0, MB0 = W0^H BV0 (jd_core.c:818-819): conj of AV^H W
+    if ((s = tsdot(S, 2, 1, 1, ld, AV, BV, W, nullptr, S.red, nullptr, st))) return s;
+    BBJD_CUDA_TRY(cudaMemcpyAsync(pin, S.red, sizeof(cplx) * 2, cudaMemcpyDeviceToHost, st));
+    if ((s = sync())) return s;
+    ws->MA[0] = std::conj(Z(pin[0]));
+    ws->MB[0] = std::conj(Z(pin[1]));
+    ws->kdim = 1;
+
+    for (int64_t iter = 0; iter < P->maxiter; ++iter) {             // jd_core.c:823
+        int64_t k = ws->kdim;
+        const int64_t locked = ws->nlock;
+        int tpos = (int)locked;
+        {
+            int64_t nkeep = minsub - locked;                        // jd_core.c:830-831
+            if (nkeep < 1) nkeep = 1;
+            if (solve_projected((int)k, (int)locked, (int)nkeep, &tpos)) {
+                res->status = BBJD_ERR_LAPACK;
+                return res->status;
+            }
+        }
+        // Ritz pair at the target position (jd_core.c:851-872)
+        const zc ta = alpha[tpos], tb = beta[tpos];
+        {
+            const int p = tpos;
+            std::vector<zc> y(p + 1);
+            y[p] = 1.0;
+            const zc *SA = ws->SA, *SB = ws->SB, *ZB = ws->ZB;
+            for (int i = p - 1; i >= 0; --i) {
+                zc acc = 0.0;
+                for (int j = i + 1; j <= p; ++j)
+                    acc += (tb * SA[i + (size_t)j * maxsub] - ta * SB[i + (size_t)j * maxsub]) * y[j];
+                const zc d = tb * SA[i + (size_t)i * maxsub] - ta * SB[i + (size_t)i * maxsub];
+                y[i] = (std::abs(d) > 1e-300) ? -acc / d : zc(0.0);
+            }
+            for (int64_t i = 0; i < k; ++i) {
+                zc acc = 0.0;
+                for (int j = 0; j <= p; ++j) acc += ZB[i + (size_t)j * maxsub] * y[j];
+                pin[i] = C(acc);
+            }
+        }
+        BBJD_CUDA_TRY(cudaMemcpyAsync(xdev, pin, sizeof(cplx) * k, cudaMemcpyHostToDevice, st));
+        // u = V x, ||u||, u /= ||u||  (jd_core.c:871-877)
+        T.begin(KC_RITZ, 16.0 * n * (k + 1.0) + 32.0 * n);
+        if ((s = update(S, (int)k, ld, V, xdev, nullptr, mk(-1, 0), mk(0, 0), mk(0, 0), nullptr, mk(0, 0),
+                        nullptr, u, dscal + SC_UNORM, nullptr, nullptr, nullptr, nullptr, st)))
+            return s;
+        if ((s = scale_by_norm(S, u, dscal + SC_UNORM, 1e-300, u, st))) return s;
+        T.end();
+        bytes_dev += 16.0 * n * (k + 1.0) + 32.0 * n;
+        // Au, Bu, r = tb Au - ta Bu, ||r||  (jd_core.c:884-890), one fused pass
+        T.begin(KC_SPMV, abytes_r);
+        s = ops->apply(u, Au, Bu, C(ta), C(tb), r, dscal + SC_RNORM);
+        T.end();
+        bytes_dev += abytes_r;
+        if (s) return s;
+        BBJD_CUDA_TRY(cudaMemcpyAsync(pin_d, dscal, sizeof(double) * 2, cudaMemcpyDeviceToHost, st));
+        if ((s = sync())) return s;
+        if (pin_d[SC_UNORM] < 1e-300) {
+            res->status = BBJD_ERR_BREAKDOWN;
+            return res->status;
+        }
+        const double res_norm = pin_d[SC_RNORM];
+        const double denom = std::abs(ta) + std::abs(tb);
+        const double rel = res_norm / (denom > 1e-300 ? denom : 1.0);
+        if (P->verbose >= 2) {
+            const zc lam = std::abs(tb) > 1e-300 ? ta / tb : ta;
+            fprintf(stderr, "  iter %3lld  kdim %3lld  locked %2lld  eig (%+.6e, %+.6e)  res %.3e\n",
+                    (long long)iter, (long long)k, (long long)locked, lam.real(), lam.imag(), rel);
+        }
+        if (rel < tol) {                                            // jd_core.c:905-932
+            const zc lam = std::abs(tb) > 1e-300 ? ta / tb : ta;
+            res->eigenvalues[res->nconv] = lam;
+            BBJD_CUDA_TRY(cudaMemcpyAsync(res->eigenvectors + (size_t)res->nconv * n, u,
+                                          sizeof(cplx) * n, cudaMemcpyDeviceToHost, st));
+            res->residuals[res->nconv] = rel;
+            res->nconv++;
+            if (P->verbose >= 1)
+                fprintf(stderr, "  *** converged #%lld: (%+.10e, %+.10e)  res %.3e  iter %lld\n",
+                        (long long)res->nconv, lam.real(), lam.imag(), rel, (long long)iter);
+            if (res->nconv >= nev) {
+                res->iters = iter + 1;
+                if ((s = sync())) return s;
+                return res->status;
+            }
+            if ((s = deflation_append((int)ws->nlock, u, Au, Bu))) return s;
+            ws->nlock++;
+            continue;
+        }
+        // correction (jd_core.c:944-972)
+        bool svdv_mode = P->inner_maxiter <= 0;
+        cplx *zc_ = z, *sc_ = sv;
+        if (!svdv_mode) {
+            if ((s = deflation_append((int)locked, u, Au, Bu))) return s;
+            if ((s = gmres((int)(ws->nlock + 1), ta, tb, r, g3))) return s;
+        } else {
+            if (ops->has_precond()) {
+                T.begin(KC_PRECOND, ops->precond_bytes(2));
+                s = ops->precond(2, r, z);                          // z = M^-1 r, s = M^-1 u
+                T.end();
+                bytes_dev += ops->precond_bytes(2);
+                if (s) return s;
+            } else {
+                zc_ = r;
+                sc_ = u;
+            }
+            if ((s = tsdot(S, 1, 2, 1, ld, u, nullptr, zc_, sc_, xdev, nullptr, st))) return s;
+            bytes_dev += 48.0 * n;
+        }
+        // thick restart (jd_core.c:975-1030)
+        if (k >= maxsub) {
+            int64_t keep = minsub < k ? minsub : k - 1;
+            if (keep < locked + 1) keep = locked + 1;
+            restarts++;
+            {
+                std::vector<cplx> zh((size_t)k * keep);
+                for (int64_t c = 0; c < keep; ++c)
+                    for (int64_t i = 0; i < k; ++i) zh[c * k + i] = C(ws->ZB[i + (size_t)c * maxsub]);
+                BBJD_CUDA_TRY(cudaMemcpyAsync(Zdev, zh.data(), sizeof(cplx) * k * keep,
+                                              cudaMemcpyHostToDevice, st));
+                // the copy must complete before zh goes out of scope
+                BBJD_CUDA_TRY(cudaStreamSynchronize(st));
+            }
+            const double gb = 16.0 * n * (double)(k + keep);
+            T.begin(KC_RESTART, 3 * gb);
+            if ((s = restart_gemm(n, (int)k, (int)keep, V, ld, Zdev, (int)k, V, st))) return s;
+            if ((s = restart_gemm(n, (int)k, (int)keep, AV, ld, Zdev, (int)k, AV, st))) return s;
+            if ((s = restart_gemm(n, (int)k, (int)keep, BV, ld, Zdev, (int)k, BV, st))) return s;
+            T.end();
+            bytes_dev += 3 * gb;
+            // rebuild W from the kept test images (jd_core.c:1002-1010)
+            for (int64_t j = 0; j < keep; ++j) {
+                cplx *wj = W + j * ld;
+                if ((s = update(S, 0, ld, nullptr, nullptr, nullptr, mk(0, 0), mk(0, 0), C(nu0), AV + j * ld,
+                                C(mu0), BV + j * ld, wj, dscal + SC_TMP, nullptr, nullptr, nullptr, nullptr, st)))
+                    return s;
+                if ((s = orthogonalize(W, ld, (int)j, wj, dscal + SC_TMP, KC_RESTART))) return s;
+                if ((s = scale_by_norm(S, wj, dscal + SC_TMP, 1e-300, wj, st))) return s;
+            }
+            // MA = W^H AV, MB = W^H BV (jd_core.c:1016-1026)
+            T.begin(KC_RESTART, 3.0 * 16.0 * n * keep);
+            if ((s = gram(S, (int)keep, W, AV, ld, gram_part, gram_G, gram_out, st))) return s;
+            if ((s = gram(S, (int)keep, W, BV, ld, gram_part, gram_G, gram_out + keep * keep, st))) return s;
+            T.end();
+            bytes_dev += 4.0 * 16.0 * n * keep;
+            {
+                std::vector<cplx> gh((size_t)2 * keep * keep);
+                BBJD_CUDA_TRY(cudaMemcpyAsync(gh.data(), gram_out, sizeof(cplx) * 2 * keep * keep,
+                                              cudaMemcpyDeviceToHost, st));
+                if ((s = sync())) return s;
+                for (int64_t c = 0; c < keep; ++c)
+                    for (int64_t i = 0; i < keep; ++i) {
+                        ws->MA[i + (size_t)c * maxsub] = Z(gh[c * keep + i]);
+                        ws->MB[i + (size_t)c * maxsub] = Z(gh[keep * keep + c * keep + i]);
+                    }
+            }
+            ws->kdim = keep;
+            k = keep;
+        }
+        // expansion (jd_core.c:1033-1048)
+        cplx *vnew = V + k * ld;
+        if (svdv_mode) {
+            if ((s = svdv(S, xdev, zc_, sc_, vnew, st))) return s;
+        } else {
+            BBJD_CUDA_TRY(cudaMemcpyAsync(vnew, g3, sizeof(cplx) * n, cudaMemcpyDeviceToDevice, st));
+        }
+        if ((s = orthogonalize(V, ld, (int)k, vnew, dscal + SC_VNORM, KC_ORTH))) return s;
+        BBJD_CUDA_TRY(cudaMemcpyAsync(pin_d + SC_VNORM, dscal + SC_VNORM, sizeof(double), cudaMemcpyDeviceToHost, st));
+        BBJD_CUDA_TRY(cudaMemcpyAsync(pin_i + FL_T, dflag + FL_T, sizeof(int), cudaMemcpyDeviceToHost, st));
+        if ((s = sync())) return s;
+        if (pin_i[FL_T]) dgks++;
+        if (pin_d[SC_VNORM] < 1e-14) {
+            std::vector<zc> rv(n);
+            for (int64_t i = 0; i < n; ++i) {
+                const double re = (double)rand() / RAND_MAX - 0.5;
+                const double im = (double)rand() / RAND_MAX - 0.5;
+                rv[i] = zc(re, im);
+            }
+            BBJD_CUDA_TRY(cudaMemcpyAsync(vnew, rv.data(), sizeof(cplx) * n, cudaMemcpyHostToDevice, st));
+            if ((s = orthogonalize(V, ld, (int)k, vnew, dscal + SC_VNORM, KC_ORTH))) return s;
+            BBJD_CUDA_TRY(cudaMemcpyAsync(pin_d + SC_VNORM, dscal + SC_VNORM, sizeof(double), cudaMemcpyDeviceToHost, st));
+            if ((s = sync())) return s;
+            if (pin_d[SC_VNORM] < 1e-14) {
+                res->iters = iter + 1;
+                res->status = BBJD_ERR_BREAKDOWN;
+                return res->status;
+            }
+        }
+        if ((s = scale_by_norm(S, vnew, dscal + SC_VNORM, 0.0, vnew, st))) return s;
+        cplx *AVk = AV + k * ld, *BVk = BV + k * ld, *wnew = W + k * ld;
+        T.begin(KC_SPMV, abytes);
+        s = ops->apply(vnew, AVk, BVk, mk(0, 0), mk(0, 0), nullptr, nullptr);  // jd_core.c:1051-1054
+        T.end();
+        bytes_dev += abytes;
+        if (s) return s;
+        // w = nu0 AV_k + mu0 BV_k, CGS2 vs W with the projected-pencil column
+        // W[:, 0:k]^H [AV_k, BV_k] taken from the same first pass over W.
+        T.begin(KC_PENCIL, 16.0 * n * (2.0 * k + 6.0));
+        if ((s = update(S, 0, ld, nullptr, nullptr, nullptr, mk(0, 0), mk(0, 0), C(nu0), AVk, C(mu0), BVk,
+                        wnew, dscal + SC_WPRE, nullptr, nullptr, nullptr, nullptr, st)))
+            return s;
+        cplx *hAB = xdev;  // [hA (k) | hB (k) | norms]
+        if ((s = tsdot(S, 1, 2, (int)k, ld, W, nullptr, AVk, BVk, hAB, nullptr, st))) return s;
+        if ((s = update(S, (int)k, ld, W, hAB, hAB + k, C(nu0), C(mu0), mk(1, 0), wnew, mk(0, 0), nullptr,
+                        wnew, dscal + SC_WNORM, nullptr, dscal + SC_WPRE, dflag + FL_W, nullptr, st)))
+            return s;
+        cplx *h2 = S.red + S.maxX;
+        if ((s = tsdot(S, 1, 1, (int)k, ld, W, nullptr, wnew, nullptr, h2, dflag + FL_W, st))) return s;
+        if ((s = update(S, (int)k, ld, W, h2, nullptr, mk(1, 0), mk(0, 0), mk(1, 0), wnew, mk(0, 0), nullptr,
+                        wnew, dscal + SC_WNORM, nullptr, nullptr, nullptr, dflag + FL_W, st)))
+            return s;
+        T.end();
+        bytes_dev += 16.0 * n * (2.0 * k + 6.0);
+        BBJD_CUDA_TRY(cudaMemcpyAsync(pin_d + SC_WNORM, dscal + SC_WNORM, sizeof(double), cudaMemcpyDeviceToHost, st));
+        BBJD_CUDA_TRY(cudaMemcpyAsync(pin_i + FL_W, dflag + FL_W, sizeof(int), cudaMemcpyDeviceToHost, st));
+        BBJD_CUDA_TRY(cudaMemcpyAsync(pin, hAB, sizeof(cplx) * 2 * k, cudaMemcpyDeviceToHost, st));
+        if ((s = sync())) return s;
+        if (pin_i[FL_W]) dgks++;
+        if (pin_d[SC_WNORM] < 1e-14) {                              // jd_core.c:1061-1064
+            BBJD_CUDA_TRY(cudaMemcpyAsync(wnew, AVk, sizeof(cplx) * n, cudaMemcpyDeviceToDevice, st));
+            if ((s = orthogonalize(W, ld, (int)k, wnew, dscal + SC_WNORM, KC_PENCIL))) return s;
+        }
+        for (int64_t i = 0; i < k; ++i) {                           // column k (rows 0..k-1)
+            ws->MA[i + (size_t)k * maxsub] = Z(pin[i]);
+            ws->MB[i + (size_t)k * maxsub] = Z(pin[k + i]);
+        }
+        if ((s = scale_by_norm(S, wnew, dscal + SC_WNORM, 1e-300, wnew, st))) return s;
+        // row k: MA[k, 0:k+1] = W_k^H AV[:, 0:k+1], MB likewise (jd_core.c:1090-1103)
+        T.begin(KC_PENCIL, 16.0 * n * (2.0 * (k + 1) + 1.0));
+        if ((s = tsdot(S, 2, 1, (int)(k + 1), ld, AV, BV, wnew, nullptr, S.red, nullptr, st))) return s;
+        T.end();
+        bytes_dev += 16.0 * n * (2.0 * (k + 1) + 1.0);
+        BBJD_CUDA_TRY(cudaMemcpyAsync(pin, S.red, sizeof(cplx) * 2 * (k + 1), cudaMemcpyDeviceToHost, st));
+        if ((s = sync())) return s;
+        for (int64_t i = 0; i <= k; ++i) {
+            ws->MA[k + (size_t)i * maxsub] = std::conj(Z(pin[i]));
+            ws->MB[k + (size_t)i * maxsub] = std::conj(Z(pin[k + 1 + i]));
+        }
+        ws->kdim = k + 1;
+        res->iters = iter + 1;
+    }
+    if (res->nconv < nev) res->status = BBJD_MAX_ITER;              // jd_core.c:1110
+    return res->status;
+}
+
+}  // namespace bbjd

@@ -1,0 +1,129 @@
+/*
+ * bbjd_gpu.h -- device-operator extension of the bbjd.h C-ABI.
+ *
+ * The reference applies A, B and the preconditioner through host callbacks
+ * (reference include/bbjd.h:101-109, bbjd.py:181-219, _bbjd_c.c:43-123).
+ * This header adds device-resident operators for block-bordered pencils
+ * (BBT: block-tridiagonal A with t dense border columns and t dense tau
+ * rows, block-diagonal B with zero tau rows) and a device preconditioner,
+ * so that a whole JDQZ solve runs on one GPU with only k x k data crossing
+ * to the host per iteration.  Nothing here has a counterpart in the
+ * reference except where a line cites one.
+ *
+ * Layout of every host or device array passed here: column-major.
+ *   blocks  Ad, Al, Au, Bd : nblk consecutive b x b column-major blocks;
+ *                            block j of Al couples block row j to block
+ *                            column j-1 (Al[0] unused), of Au to j+1
+ *                            (Au[nblk-1] unused).
+ *   E                       : nb x t column-major (ld = nb), A[0:nb, nb:n]
+ *   F                       : t x n column-major (ld = t),   A[nb:n, 0:n]
+ * with nb = nblk * b and n = nb + t.  Device vectors are contiguous,
+ * 16-byte aligned complex128 (or complex64 where stated).
+ */
+#ifndef BBJD_GPU_H
+#define BBJD_GPU_H
+
+#include "bbjd.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct bbjd_bbt_matrix bbjd_bbt_matrix;   /* opaque: A and B on one device */
+typedef struct bbjd_precond    bbjd_precond;      /* opaque: device M^-1          */
+
+enum { BBJD_FP64 = 0, BBJD_MIXED = 1 };
+enum { BBJD_PC_NONE = 0, BBJD_PC_BBT_LU = 1, BBJD_PC_BLOCK_JACOBI = 2 };
+
+/* Copy a BBT pencil to the current device.  from_host = 1: pointers are host
+ * memory; 0: device memory (copied).  b must be 8, 16 or 32. */
+bbjd_status bbjd_bbt_create(bbjd_int b, bbjd_int nblk, bbjd_int t,
+                            const bbjd_zomplex *Ad, const bbjd_zomplex *Al,
+                            const bbjd_zomplex *Au, const bbjd_zomplex *E,
+                            const bbjd_zomplex *F, const bbjd_zomplex *Bd,
+                            int from_host, bbjd_bbt_matrix **out);
+void        bbjd_bbt_free(bbjd_bbt_matrix *m);
+bbjd_int    bbjd_bbt_n(const bbjd_bbt_matrix *m);
+/* Algorithmic bytes one fused A,B product reads and writes (HBM roofline). */
+double      bbjd_bbt_matvec_bytes(const bbjd_bbt_matrix *m);
+
+/* yA = A x and yB = B x on device vectors, one fused pass (replaces the
+ * matvec_A / matvec_B callbacks, reference jd_core.c:884-885). */
+bbjd_status bbjd_bbt_matvec(const bbjd_bbt_matrix *m, const bbjd_zomplex *x,
+                            bbjd_zomplex *yA, bbjd_zomplex *yB, void *stream);
+
+/* Device preconditioner for A - sigma B.
+ *   kind BBJD_PC_BBT_LU       : exact block-bordered LU (block cyclic
+ *                               reduction of the block-tridiagonal interior,
+ *                               t x t Schur complement for the border);
+ *   kind BBJD_PC_BLOCK_JACOBI : inverses of the diagonal blocks and of the
+ *                               t x t tau corner.
+ * precision BBJD_MIXED stores the factors in complex64. */
+bbjd_status bbjd_precond_create(const bbjd_bbt_matrix *m, bbjd_zomplex sigma,
+                                int kind, int precision, bbjd_precond **out);
+void        bbjd_precond_free(bbjd_precond *pc);
+double      bbjd_precond_solve_bytes(const bbjd_precond *pc, int nrhs);
+double      bbjd_precond_factor_seconds(const bbjd_precond *pc);
+/* x[:, j] = M^-1 r[:, j] for nrhs <= 2 device vectors stored with stride n. */
+bbjd_status bbjd_precond_solve(const bbjd_precond *pc, int nrhs,
+                               const bbjd_zomplex *r, bbjd_zomplex *x, void *stream);
+
+/* Options and instrumentation of a device solve. */
+typedef struct {
+    int     precision;          /* BBJD_FP64 (default) or BBJD_MIXED            */
+    int     record_timing;      /* 1: fill the timing fields (adds syncs)       */
+    void   *stream;             /* cudaStream_t, NULL = a private stream        */
+    /* out */
+    double  seconds_total;      /* wall time of the solve                       */
+    double  seconds_qz;         /* host projected QZ + reorder                  */
+    double  seconds_device;     /* device time (CUDA events, summed)            */
+    double  seconds_restart;    /* device time spent in thick restarts          */
+    double  bytes_device;       /* algorithmic HBM bytes of the device work     */
+    int64_t kernel_launches;    /* kernels this library launched                */
+    int64_t dgks_passes;        /* second CGS passes taken                      */
+    int64_t restarts;
+    double  kernel_ms[8];       /* per kernel class: spmv, orth, pencil, ritz,
+                                   precond, restart, small, gmres (if timed)    */
+    double  kernel_bytes[8];
+    int64_t kernel_calls[8];
+} bbjd_device_ext;
+
+void bbjd_device_ext_init(bbjd_device_ext *ext);
+
+/* JDQZ with device operators: params->matvec_A/B/precond/op_data are
+ * ignored; A and B are `m`, the preconditioner is `pc` (NULL = identity).
+ * ws comes from bbjd_workspace_alloc with the same params.  Same algorithm,
+ * constants and result contract as bbjd_solve. */
+bbjd_status bbjd_solve_device(const bbjd_params *params, bbjd_device_ext *ext,
+                              const bbjd_bbt_matrix *m, const bbjd_precond *pc,
+                              bbjd_workspace *ws, bbjd_result *result);
+
+/* ---- device kernels exposed for parity tests (device pointers) ---------- */
+
+/* CGS + DGKS of v (length n) against the k columns of Q (ld = ldq); returns
+ * ||v|| afterwards through *norm_out (host).  reference jd_core.c:207-241 */
+bbjd_status bbjd_dev_orthogonalize(bbjd_int n, bbjd_int k, const bbjd_zomplex *Q,
+                                   bbjd_int ldq, bbjd_zomplex *v, double *norm_out,
+                                   int *second_pass_out, void *stream);
+
+/* out = X[:, 0:k] * Z[0:k, 0:keep]  (X, out ld = ldx; Z host k x keep col-major,
+ * ldz).  Thick-restart compression, reference jd_core.c:989-999. */
+bbjd_status bbjd_dev_restart_gemm(bbjd_int n, bbjd_int k, bbjd_int keep,
+                                  const bbjd_zomplex *X, bbjd_int ldx,
+                                  const bbjd_zomplex *Z_host, bbjd_int ldz,
+                                  bbjd_zomplex *out, void *stream);
+
+/* C (host, keep x keep, ldc) = X^H Y for device X, Y (n x keep, ld = ldx).
+ * reference jd_core.c:1020-1025 */
+bbjd_status bbjd_dev_gram(bbjd_int n, bbjd_int keep, const bbjd_zomplex *X,
+                          const bbjd_zomplex *Y, bbjd_int ldx,
+                          bbjd_zomplex *C_host, bbjd_int ldc, void *stream);
+
+/* Library version / build string. */
+const char *bbjd_gpu_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BBJD_GPU_H */

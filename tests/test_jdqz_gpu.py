@@ -1,0 +1,109 @@
+"""End-to-end parity of the device JDQZ against the reference's own results
+(tests/golden, produced by running the reference) and against ARPACK, on
+the block-bordered pencils the reference targets.  See tests/parity.py for
+the criteria and their tolerances."""
+import os
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+from bbjd_b200 import DevicePencil, DevicePreconditioner, jdqz, make_pencil, start_vector
+from tests.parity import EIG_ATOL, assert_no_duplicates, match_set
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def _load(name):
+    return dict(np.load(os.path.join(GOLDEN, name + ".npz"), allow_pickle=False))
+
+
+def _check_pairs(P, ev, evecs, g, tol=1e-10):
+    A, B = P.to_csc("A"), P.to_csc("B")
+    nA, nB = sp.linalg.norm(A), sp.linalg.norm(B)
+    for lam, x in zip(ev, evecs.T):
+        r = A @ x - lam * (B @ x)
+        # normalised residual of the north-star acceptance test
+        assert np.linalg.norm(r) / ((nA + abs(lam) * nB) * np.linalg.norm(x)) < tol
+        # the reference test suite's unscaled measure (tests/test_bbjd.py:96-98)
+        assert np.linalg.norm(r) / np.linalg.norm(x) < 1e-8
+    ref_set = np.concatenate([g["eigenvalues"], g["arpack"]])
+    assert match_set(ev, ref_set).max() < EIG_ATOL
+    assert_no_duplicates(ev)
+
+
+@pytest.mark.parametrize("name", ["bbt_n516", "bbt_n1056_b32", "bbt_n4104"])
+def test_device_jdqz_matches_reference(name):
+    g = _load(name)
+    P = make_pencil(int(g["b"]), int(g["nblk"]), int(g["t"]), seed=int(g["seed"]))
+    sigma = complex(g["sigma"])
+    ev, evecs, info = jdqz(P, k=int(g["k"]), sigma=sigma, tol=1e-10, maxiter=int(g["maxiter"]),
+                           maxsub=int(g["maxsub"]), minsub=int(g["minsub"]),
+                           preconditioner="exact", v0=start_vector(P.n, int(g["seed"]) + 1),
+                           return_info=True)
+    assert info["nconv"] == int(g["k"]) and info["status"] == 0
+    _check_pairs(P, ev, evecs, g)
+    # same eigenvalues as the reference's own run
+    assert match_set(ev, g["eigenvalues"]).max() < EIG_ATOL
+    assert match_set(g["eigenvalues"], ev).max() < EIG_ATOL
+    # same algorithm: the iteration count differs from the reference's only
+    # through rounding (the reference itself varies by ~5% with BLAS threads)
+    assert abs(info["iters"] - int(g["iters"])) <= max(10, 0.25 * int(g["iters"]))
+    # solver-measure residuals below tol, reported per pair
+    assert np.all(info["residuals"] < 1e-10)
+
+
+def test_device_jdqz_gmres_matches_reference():
+    g = _load("bbt_n516_gmres")
+    P = make_pencil(int(g["b"]), int(g["nblk"]), int(g["t"]), seed=int(g["seed"]))
+    sigma = complex(g["sigma"])
+    dev = DevicePencil(P)
+    approx = DevicePreconditioner(dev, sigma + complex(g["pc_shift"]), "exact")
+    ev, evecs, info = jdqz(dev, k=int(g["k"]), sigma=sigma, tol=1e-10, maxiter=int(g["maxiter"]),
+                           maxsub=int(g["maxsub"]), minsub=int(g["minsub"]),
+                           inner_maxiter=int(g["inner_maxiter"]), inner_tol=float(g["inner_tol"]),
+                           preconditioner=approx, v0=start_vector(P.n, 1), return_info=True)
+    assert info["nconv"] == int(g["k"])
+    _check_pairs(P, ev, evecs, g)
+    assert match_set(ev, g["eigenvalues"]).max() < EIG_ATOL
+    assert abs(info["iters"] - int(g["iters"])) <= max(10, 0.25 * int(g["iters"]))
+
+
+def test_device_jdqz_block_jacobi_gmres():
+    """The inner-GMRES configuration's preconditioner on a small pencil."""
+    g = _load("bbt_n1056_b32")
+    P = make_pencil(int(g["b"]), int(g["nblk"]), int(g["t"]), seed=int(g["seed"]))
+    ev, evecs, info = jdqz(P, k=3, sigma=3.0, tol=1e-10, maxiter=1500, maxsub=40, minsub=16,
+                           inner_maxiter=50, inner_tol=1e-3, preconditioner="block_jacobi",
+                           v0=start_vector(P.n, 4), return_info=True)
+    assert info["nconv"] == 3
+    _check_pairs(P, ev, evecs, g)
+    # the three nearest to sigma are the first three of the ARPACK set
+    assert match_set(ev, g["arpack"][:4]).max() < EIG_ATOL
+
+
+def test_device_without_preconditioner_and_random_start():
+    P = make_pencil(8, 16, 2, seed=9)
+    ev, evecs, info = jdqz(P, k=2, sigma=3.0, tol=1e-9, maxiter=400, return_info=True)
+    assert info["nconv"] == 2
+    A, B = P.to_csc("A"), P.to_csc("B")
+    for lam, x in zip(ev, evecs.T):
+        assert np.linalg.norm(A @ x - lam * (B @ x)) / np.linalg.norm(x) < 1e-7
+
+
+def test_device_v0_length_checked():
+    P = make_pencil(8, 4, 2)
+    with pytest.raises(ValueError):
+        jdqz(P, k=1, sigma=3.0, preconditioner="exact", v0=np.ones(P.n - 1))
+
+
+def test_device_stats_reported():
+    P = make_pencil(16, 64, 8, seed=0)
+    ev, evecs, info = jdqz(P, k=2, sigma=3.0, preconditioner="exact", maxsub=20, minsub=8,
+                           maxiter=500, v0=start_vector(P.n, 1), return_info=True, timing=True)
+    d = info["device"]
+    assert info["nconv"] == 2
+    assert d["kernel_launches"] > 0 and d["bytes_device"] > 0
+    assert d["kernels"]["spmv"]["calls"] > 0 and d["kernels"]["spmv"]["ms"] > 0
+    assert d["restarts"] >= 1

@@ -1,0 +1,166 @@
+"""Kernel-level parity of the device kernels against host references, through
+the C-ABI.  Integer-free floating-point work: tolerances are stated per test
+(FP64 throughout; reductions differ from numpy only in summation order)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+from scipy.sparse.linalg import splu
+
+from bbjd_b200 import DevicePencil, DevicePreconditioner, _lib, make_pencil
+from oracle import jdqz_np
+
+pytestmark = pytest.mark.gpu
+
+
+def _dev(a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a)).to("cuda")
+
+
+def _host(t):
+    return t.cpu().numpy()
+
+
+def _rand(n, seed):
+    rng = np.random.default_rng(seed)
+    return rng.standard_normal(n) + 1j * rng.standard_normal(n)
+
+
+SPMV_CASES = [(8, 64, 4), (16, 256, 8), (16, 33, 8), (32, 100, 64), (32, 7, 32), (16, 40, 0),
+              (8, 1, 3), (32, 31, 96)]
+
+
+@pytest.mark.parametrize("b,nblk,t", SPMV_CASES)
+def test_bbt_matvec_matches_host(b, nblk, t):
+    import torch
+    P = make_pencil(b, nblk, t, seed=11)
+    dev = DevicePencil(P)
+    x = _rand(P.n, 3)
+    xd = _dev(x)
+    yA = torch.empty_like(xd)
+    yB = torch.empty_like(xd)
+    lib = _lib.load()
+    assert lib.bbjd_bbt_matvec(dev.handle, xd.data_ptr(), yA.data_ptr(), yB.data_ptr(), None) == 0
+    torch.cuda.synchronize()
+    refA, refB = P.matvec_A(x), P.matvec_B(x)
+    # FP64, different summation order: 1e-13 relative to the row scale
+    scale = np.abs(x).max() * (np.abs(P.Ad).max() * 3 * b + 1)
+    assert np.abs(_host(yA) - refA).max() < 1e-13 * scale
+    assert np.abs(_host(yB) - refB).max() < 1e-13 * scale
+    assert np.all(_host(yB)[P.nb:] == 0)
+
+
+LU_CASES = [(8, 64, 4), (16, 33, 8), (16, 256, 8), (32, 100, 64), (8, 1, 2), (8, 2, 0), (32, 3, 32)]
+
+
+@pytest.mark.parametrize("b,nblk,t", LU_CASES)
+@pytest.mark.parametrize("nrhs", [1, 2])
+def test_bbt_lu_solve_matches_scipy(b, nblk, t, nrhs):
+    import torch
+    P = make_pencil(b, nblk, t, seed=5)
+    sigma = 3.0 + 0.25j
+    dev = DevicePencil(P)
+    pc = DevicePreconditioner(dev, sigma, "exact")
+    M = (P.to_csc("A") - sigma * P.to_csc("B")).tocsc()
+    r = np.stack([_rand(P.n, 10 + q) for q in range(nrhs)])
+    rd = _dev(r)
+    xd = torch.empty_like(rd)
+    lib = _lib.load()
+    assert lib.bbjd_precond_solve(pc.handle, nrhs, rd.data_ptr(), xd.data_ptr(), None) == 0
+    torch.cuda.synchronize()
+    x = _host(xd)
+    ref = splu(M)
+    for q in range(nrhs):
+        # backward error of the device solve, and agreement with SuperLU
+        res = np.linalg.norm(M @ x[q] - r[q]) / (sp.linalg.norm(M) * np.linalg.norm(x[q]))
+        assert res < 1e-13
+        xs = ref.solve(r[q])
+        assert np.linalg.norm(x[q] - xs) / np.linalg.norm(xs) < 1e-9
+
+
+def test_bbt_lu_in_place():
+    import torch
+    P = make_pencil(16, 50, 8, seed=1)
+    dev = DevicePencil(P)
+    pc = DevicePreconditioner(dev, 2.0, "exact")
+    r = _rand(P.n, 4)
+    rd = _dev(r)
+    lib = _lib.load()
+    assert lib.bbjd_precond_solve(pc.handle, 1, rd.data_ptr(), rd.data_ptr(), None) == 0
+    torch.cuda.synchronize()
+    M = (P.to_csc("A") - 2.0 * P.to_csc("B")).tocsc()
+    assert np.linalg.norm(M @ _host(rd) - r) / np.linalg.norm(r) < 1e-11
+
+
+@pytest.mark.parametrize("b,nblk,t", [(8, 20, 4), (32, 10, 64)])
+def test_block_jacobi_matches_host(b, nblk, t):
+    import torch
+    P = make_pencil(b, nblk, t, seed=2)
+    sigma = 3.0
+    dev = DevicePencil(P)
+    pc = DevicePreconditioner(dev, sigma, "block_jacobi")
+    r = _rand(P.n, 1)
+    rd = _dev(r)
+    xd = torch.empty_like(rd)
+    lib = _lib.load()
+    assert lib.bbjd_precond_solve(pc.handle, 1, rd.data_ptr(), xd.data_ptr(), None) == 0
+    torch.cuda.synchronize()
+    D = P.Ad - sigma * P.Bd
+    ref = np.concatenate([np.linalg.solve(D[j], r[j * b:(j + 1) * b]) for j in range(nblk)] +
+                         ([np.linalg.solve(P.F[:, P.nb:], r[P.nb:])] if t else []))
+    assert np.linalg.norm(_host(xd) - ref) / np.linalg.norm(ref) < 1e-12
+
+
+@pytest.mark.parametrize("n,k", [(1000, 0), (1000, 1), (4104, 37), (100003, 200), (50, 50)])
+def test_orthogonalize_matches_oracle(n, k):
+    import torch
+    rng = np.random.default_rng(n + k)
+    Q = np.linalg.qr(rng.standard_normal((n, max(k, 1))) + 1j * rng.standard_normal((n, max(k, 1))))[0][:, :k]
+    v = _rand(n, 9) + (Q @ _rand(k, 8) * 10 if k else 0)
+    Qd = _dev(np.asfortranarray(Q).T.copy()) if k else _dev(np.zeros(1, np.complex128))
+    vd = _dev(v)
+    nrm = C.c_double()
+    second = C.c_int()
+    lib = _lib.load()
+    assert lib.bbjd_dev_orthogonalize(n, k, Qd.data_ptr(), n, vd.data_ptr(), C.byref(nrm),
+                                      C.byref(second), None) == 0
+    vv = v.copy()
+    ref_nrm = jdqz_np.block_orthogonalize(Q, vv)
+    assert abs(nrm.value - ref_nrm) < 1e-12 * max(1.0, ref_nrm)
+    assert np.linalg.norm(_host(vd) - vv) < 1e-12 * np.linalg.norm(v)
+    if k:
+        # the large component along Q forces the DGKS re-pass
+        assert second.value == 1
+        assert np.abs(Q.conj().T @ _host(vd)).max() < 1e-12 * np.linalg.norm(v)
+
+
+@pytest.mark.parametrize("n,k,keep", [(1000, 40, 20), (100000, 200, 80), (777, 30, 29), (5000, 150, 128)])
+def test_restart_gemm_matches_numpy(n, k, keep):
+    import torch
+    rng = np.random.default_rng(1)
+    X = rng.standard_normal((n, k)) + 1j * rng.standard_normal((n, k))
+    Z = np.asfortranarray(rng.standard_normal((k, keep)) + 1j * rng.standard_normal((k, keep)))
+    Xd = _dev(X.T.copy())        # column-major n x k
+    lib = _lib.load()
+    outd = torch.empty_like(Xd) if keep > 128 else Xd   # in place when one column tile
+    zh = np.asfortranarray(Z)
+    assert lib.bbjd_dev_restart_gemm(n, k, keep, Xd.data_ptr(), n, zh.ctypes.data, k,
+                                     outd.data_ptr(), None) == 0
+    out = _host(outd).reshape(-1, n).T[:, :keep]
+    ref = X @ Z
+    assert np.abs(out - ref).max() < 1e-12 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("n,keep", [(1000, 20), (100000, 80), (3000, 100)])
+def test_gram_matches_numpy(n, keep):
+    rng = np.random.default_rng(2)
+    X = rng.standard_normal((n, keep)) + 1j * rng.standard_normal((n, keep))
+    Y = rng.standard_normal((n, keep)) + 1j * rng.standard_normal((n, keep))
+    Xd, Yd = _dev(X.T.copy()), _dev(Y.T.copy())
+    Cm = np.zeros((keep, keep), np.complex128, order="F")
+    lib = _lib.load()
+    assert lib.bbjd_dev_gram(n, keep, Xd.data_ptr(), Yd.data_ptr(), n, Cm.ctypes.data, keep, None) == 0
+    ref = X.conj().T @ Y
+    assert np.abs(Cm - ref).max() < 1e-12 * np.abs(ref).max()
