@@ -42,21 +42,29 @@ _TARGET_MAP = {
 class DevicePencil:
     """A block-bordered pencil resident on the current GPU (bbjd_bbt_create)."""
 
-    def __init__(self, pencil: BBTPencil):
-        pencil.validate()
+    def __init__(self, pencil: BBTPencil | None = None, *, arrays: dict | None = None,
+                 b: int = 0, nblk: int = 0, t: int = 0):
+        """Upload ``pencil`` (host layout), or ``arrays`` already in the
+        C-ABI's column-major layout (``BBTPencil.device_arrays()``, e.g. in
+        pinned memory) with their ``b``, ``nblk``, ``t``."""
         lib = _lib.load()
-        arrs = pencil.device_arrays()
+        if pencil is not None:
+            pencil.validate()
+            arrays = pencil.device_arrays()
+            b, nblk, t = pencil.b, pencil.nblk, pencil.t
+        elif arrays is None:
+            raise ValueError("pass a BBTPencil or its device-layout arrays")
+        addr = lambda a: a.data_ptr() if hasattr(a, "data_ptr") else _lib.ptr(a)  # noqa: E731
         h = C.c_void_p()
-        st = lib.bbjd_bbt_create(pencil.b, pencil.nblk, pencil.t,
-                                 _lib.ptr(arrs["Ad"]), _lib.ptr(arrs["Al"]), _lib.ptr(arrs["Au"]),
-                                 _lib.ptr(arrs["E"]) if pencil.t else None,
-                                 _lib.ptr(arrs["FT"]) if pencil.t else None,
-                                 _lib.ptr(arrs["Bd"]), 1, C.byref(h))
+        st = lib.bbjd_bbt_create(b, nblk, t, addr(arrays["Ad"]), addr(arrays["Al"]),
+                                 addr(arrays["Au"]), addr(arrays["E"]) if t else None,
+                                 addr(arrays["FT"]) if t else None, addr(arrays["Bd"]), 1,
+                                 C.byref(h))
         if st != 0:
             raise RuntimeError(f"bbjd_bbt_create failed: {_lib.STATUS_MSG.get(st, st)}")
         self.handle = h
-        self.b, self.nblk, self.t = pencil.b, pencil.nblk, pencil.t
-        self.n = pencil.n
+        self.b, self.nblk, self.t = b, nblk, t
+        self.n = nblk * b + t
         self.shape = (self.n, self.n)
         self._lib = lib
 
@@ -219,8 +227,13 @@ def jdqz_c(n, nev, sigma, target, matvec_A, matvec_B, precond_solve, tol=1e-10, 
     return ev, evecs, resid, int(res.nconv), int(res.iters), int(status)
 
 
+_PROJECTED = {"auto": 0, "qz": 1, "schur": 2}
+_LOCK = {"robust": 0, "reference": 1}
+
+
 def _solve_device(dev: DevicePencil, pc, k, sigma, target, tol, maxiter, maxsub, minsub,
-                  inner_maxiter, inner_tol, v0, verbose, timing):
+                  inner_maxiter, inner_tol, v0, verbose, timing, projected="auto",
+                  lock="robust"):
     lib = _lib.load()
     n = dev.n
     p = _lib.Params()
@@ -236,6 +249,12 @@ def _solve_device(dev: DevicePencil, pc, k, sigma, target, tol, maxiter, maxsub,
     ext = _lib.DeviceExt()
     lib.bbjd_device_ext_init(C.byref(ext))
     ext.record_timing = 1 if timing else 0
+    if projected not in _PROJECTED:
+        raise ValueError(f"projected must be one of {list(_PROJECTED)}")
+    ext.projected = _PROJECTED[projected]
+    if lock not in _LOCK:
+        raise ValueError(f"lock must be one of {list(_LOCK)}")
+    ext.lock_rule = _LOCK[lock]
     ws = lib.bbjd_workspace_alloc(C.byref(p))
     if not ws:
         raise MemoryError("bbjd_workspace_alloc failed (device memory)")
@@ -254,6 +273,7 @@ def _solve_device(dev: DevicePencil, pc, k, sigma, target, tol, maxiter, maxsub,
         "seconds_device": ext.seconds_device, "seconds_restart": ext.seconds_restart,
         "bytes_device": ext.bytes_device, "kernel_launches": int(ext.kernel_launches),
         "dgks_passes": int(ext.dgks_passes), "restarts": int(ext.restarts),
+        "duplicates": int(ext.duplicates),
         "kernels": {name: {"ms": ext.kernel_ms[i], "bytes": ext.kernel_bytes[i],
                            "calls": int(ext.kernel_calls[i])}
                     for i, name in enumerate(_lib.KERNEL_CLASSES)},
@@ -278,6 +298,8 @@ def jdqz(
     verbose: int = 0,
     return_info: bool = False,
     timing: bool = False,
+    projected: str = "auto",
+    lock: str = "robust",
 ):
     """Jacobi-Davidson QZ for ``A x = lambda B x``, the eigenvalues nearest
     ``sigma`` first.  Parameters, defaults, returns and errors are those of
@@ -289,6 +311,16 @@ def jdqz(
     maxsub 0 means max(3k + 10, 40) capped at n; minsub 0 means
     max(2k + 5, 20) (the values the reference's C core uses,
     jd_core.c:95-98 and 750-752).
+
+    Device path only: ``timing`` records per-kernel-class CUDA-event times
+    in ``info['device']``; ``projected`` picks the projected eigensolver
+    ('qz': ZGGES + ZTGSEN as the reference; 'schur': the harmonic standard
+    form, same deflating subspaces, ~4x cheaper; 'auto': 'schur' for the
+    'nearest' and 'SM' targets).  The callback path always uses 'qz'.
+    ``lock`` picks how converged values are recognised: 'robust' (a relative
+    window and an eigenvector-angle test, so an ill-conditioned eigenvalue is
+    not returned twice) or 'reference' (the reference's absolute 100 tol
+    window, jd_core.c:369, 439).
     """
     if which not in _TARGET_MAP:
         raise ValueError(f"which must be one of {list(_TARGET_MAP.keys())}; got {which!r}")
@@ -318,7 +350,7 @@ def jdqz(
         try:
             ev, evecs, resid, nconv, iters, status, stats = _solve_device(
                 dev, pc, k, sigma, target, tol, maxiter, maxsub, minsub, inner_maxiter,
-                inner_tol, v0, verbose, timing)
+                inner_tol, v0, verbose, timing, projected, lock)
         finally:
             if own_pc:
                 pc.close()

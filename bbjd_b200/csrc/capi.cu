@@ -137,6 +137,7 @@ static bbjd_status run_engine(const bbjd_params *p, bbjd_workspace *ws, bbjd_res
         ext->kernel_launches = g_launches.load() - l0;
         ext->dgks_passes = E.dgks;
         ext->restarts = E.restarts;
+        ext->duplicates = E.duplicates;
         double dev = 0.0;
         E.T.flush();
         for (int c = 0; c < KC_N && c < 8; ++c) {

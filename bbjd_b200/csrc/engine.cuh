@@ -87,9 +87,25 @@ struct Engine {
     std::vector<zc> alpha, beta, zwork;
     std::vector<double> rwork;
     std::vector<int> bwork, sel, iwork;
+    // harmonic standard-form projected solve: C = nu0 MA + mu0 MB,
+    // H = C^-1 MB = Q T Q^H (ld = maxsub); omega = eig(H)
+    int proj_mode = BBJD_PROJ_QZ;
+    bool schur_step = false;          // the last projected solve used the Schur form
+    std::vector<zc> hC, hT, hQ, tau, omega;
+    std::vector<int> ipiv;
     double qz_seconds = 0;
-    long long dgks = 0, restarts = 0;
+    long long dgks = 0, restarts = 0, duplicates = 0;
     double bytes_dev = 0;
+    // locked eigenvalues and the window within which a Ritz value matches one
+    struct Lock { zc value; double window; };
+    std::vector<Lock> locks;
+    int lock_rule = BBJD_LOCK_ROBUST;
+    double lock_rel = 1e-6;
+    bool is_locked(zc lam) const {
+        for (const auto &l : locks)
+            if (std::abs(lam - l.value) < l.window) return true;
+        return false;
+    }
 
     bbjd_status init(const bbjd_params *p, bbjd_workspace *w, bbjd_result *r, bbjd_device_ext *e,
                      Operators *o, cudaStream_t stream);
@@ -103,7 +119,11 @@ struct Engine {
     bbjd_status deflation_append(int j, const cplx *u, const cplx *Au_, const cplx *Bu_);
     bbjd_status gmres(int ndefl, zc ta, zc tb, const cplx *r, cplx *z);
     int solve_projected(int k, int locked, int nkeep, int *target_pos);
+    int solve_projected_schur(int k, int nkeep, bool reorder, int *target_pos);
+    void select_and_scan(int k, int nkeep, int *target_pos);
+    void ritz_coefficients(int k, int p, zc ta, zc tb, cplx *x);
     bbjd_status sync();
+    void second_pass_bytes(int cls, int k);
 };
 
 }  // namespace bbjd

@@ -26,6 +26,19 @@ void scipy_ztgsen_(const int *ijob, const int *wantq, const int *wantz, const in
                    bbjd_zomplex *alpha, bbjd_zomplex *beta, bbjd_zomplex *q, const int *ldq,
                    bbjd_zomplex *z, const int *ldz, int *m, double *pl, double *pr, double *dif,
                    bbjd_zomplex *work, const int *lwork, int *iwork, const int *liwork, int *info);
+void scipy_zgetrf_(const int *m, const int *n, bbjd_zomplex *a, const int *lda, int *ipiv, int *info);
+void scipy_zgetrs_(const char *trans, const int *n, const int *nrhs, const bbjd_zomplex *a,
+                   const int *lda, const int *ipiv, bbjd_zomplex *b, const int *ldb, int *info);
+void scipy_zgehrd_(const int *n, const int *ilo, const int *ihi, bbjd_zomplex *a, const int *lda,
+                   bbjd_zomplex *tau, bbjd_zomplex *work, const int *lwork, int *info);
+void scipy_zunghr_(const int *n, const int *ilo, const int *ihi, bbjd_zomplex *a, const int *lda,
+                   const bbjd_zomplex *tau, bbjd_zomplex *work, const int *lwork, int *info);
+void scipy_zhseqr_(const char *job, const char *compz, const int *n, const int *ilo, const int *ihi,
+                   bbjd_zomplex *h, const int *ldh, bbjd_zomplex *w, bbjd_zomplex *z, const int *ldz,
+                   bbjd_zomplex *work, const int *lwork, int *info);
+void scipy_ztrsen_(const char *job, const char *compq, const int *select, const int *n,
+                   bbjd_zomplex *t, const int *ldt, bbjd_zomplex *q, const int *ldq, bbjd_zomplex *w,
+                   int *m, double *s, double *sep, bbjd_zomplex *work, const int *lwork, int *info);
 }
 
 namespace bbjd {
@@ -132,6 +145,11 @@ bbjd_status Engine::init(const bbjd_params *p, bbjd_workspace *w, bbjd_result *r
     rwork.resize(8 * maxsub);
     bwork.resize(maxsub);
     sel.resize(maxsub);
+    hC.resize((size_t)maxsub * maxsub);
+    tau.resize(maxsub);
+    omega.resize(maxsub);
+    ipiv.resize(maxsub);
+    zwork.resize(64 * (size_t)maxsub + 64);
     return BBJD_SUCCESS;
 }
 
@@ -145,6 +163,13 @@ void Engine::release() {
     cudaFreeHost(pin); cudaFreeHost(pin_d); cudaFreeHost(pin_i);
     if (own_stream && st) cudaStreamDestroy(st);
     st = nullptr;
+}
+
+// A DGKS re-pass ran (the device flag was read back): count its traffic.
+void Engine::second_pass_bytes(int cls, int k) {
+    const double b = 16.0 * (double)n * (2.0 * k + 3.0);
+    T.bytes[cls] += b;
+    bytes_dev += b;
 }
 
 bbjd_status Engine::sync() {
@@ -254,26 +279,7 @@ int Engine::solve_projected(int k, int locked, int nkeep, int *target_pos) {
     scipy_zgges_("V", "V", "N", nullptr, &bk, SA, &lda, SB, &lda, &sdim, alpha.data(), beta.data(),
                  ZA, &lda, ZB, &lda, zwork.data(), &lwork, rwork.data(), bwork.data(), &info);
     if (info) return -1;
-    const zc *conv = res->eigenvalues;
-    const int64_t nconv = res->nconv;
-    std::fill(sel.begin(), sel.begin() + k, 0);
-    for (int i = 0; i < k; ++i) {                                   // jd_core.c:365-374
-        if (std::abs(beta[i]) < 1e-300) continue;
-        const zc lam = alpha[i] / beta[i];
-        for (int64_t c = 0; c < nconv; ++c)
-            if (std::abs(lam - conv[c]) < tol * 100) { sel[i] = 1; break; }
-    }
-    for (int pick = 0; pick < nkeep; ++pick) {                      // jd_core.c:379-401
-        int tidx = -1;
-        double best = DBL_MAX;
-        for (int i = 0; i < k; ++i) {
-            if (sel[i] || std::abs(beta[i]) < 1e-300) continue;
-            const double v = target_value(alpha[i] / beta[i], sigma, target);
-            if (v < best) { best = v; tidx = i; }
-        }
-        if (tidx < 0) break;
-        sel[tidx] = 1;
-    }
+    select_and_scan(k, nkeep, nullptr);
     int nsel = 0;
     for (int i = 0; i < k; ++i) nsel += sel[i];
     if (nsel > 0) {                                                 // jd_core.c:407-425
@@ -292,21 +298,135 @@ int Engine::solve_projected(int k, int locked, int nkeep, int *target_pos) {
                       iwork.data(), &tli, &info);
         if (info) return -1;
     }
-    int tpos = 0;                                                   // jd_core.c:430-458
+    select_and_scan(k, 0, target_pos);
+    schur_step = false;
+    qz_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return 0;
+}
+
+// SELECT (locked values plus the nkeep best unconverged, reference
+// jd_core.c:365-401) when target_pos == nullptr; otherwise the target scan
+// over all positions (reference jd_core.c:430-458).  Values are
+// alpha[i] / beta[i]; |beta| < 1e-300 marks an infinite value.
+void Engine::select_and_scan(int k, int nkeep, int *target_pos) {
+    auto is_conv = [&](zc lam) { return is_locked(lam); };
+    if (!target_pos) {
+        std::fill(sel.begin(), sel.begin() + k, 0);
+        for (int i = 0; i < k; ++i) {
+            if (std::abs(beta[i]) < 1e-300) continue;
+            if (is_conv(alpha[i] / beta[i])) sel[i] = 1;
+        }
+        for (int pick = 0; pick < nkeep; ++pick) {
+            int tidx = -1;
+            double best = DBL_MAX;
+            for (int i = 0; i < k; ++i) {
+                if (sel[i] || std::abs(beta[i]) < 1e-300) continue;
+                const double v = target_value(alpha[i] / beta[i], sigma, target);
+                if (v < best) { best = v; tidx = i; }
+            }
+            if (tidx < 0) break;
+            sel[tidx] = 1;
+        }
+        return;
+    }
+    int tpos = 0;
     double best = DBL_MAX;
     for (int i = 0; i < k; ++i) {
         if (std::abs(beta[i]) < 1e-300) continue;
         const zc lam = alpha[i] / beta[i];
-        bool is_conv = false;
-        for (int64_t c = 0; c < nconv; ++c)
-            if (std::abs(lam - conv[c]) < tol * 100) { is_conv = true; break; }
-        if (is_conv) continue;
+        if (is_conv(lam)) continue;
         const double v = target_value(lam, sigma, target);
         if (v < best) { best = v; tpos = i; }
     }
     *target_pos = tpos;
+}
+
+// Harmonic standard form of the projected pencil.  With C = nu0 MA + mu0 MB
+// (nonsingular), MA x = lambda MB x  <=>  H x = omega x,  H = C^-1 MB,
+// omega = 1 / (nu0 lambda + mu0).  The Schur vectors Q of H span the same
+// nested right deflating subspaces as ZB of the generalized Schur form, so Q
+// takes ZB's place in the Ritz vector and the thick restart.  Eigenvalues go
+// to alpha (lambda) and beta (1; 0 for an infinite lambda, omega = 0).
+// Returns 1 when C is singular (the caller falls back to QZ), -1 on a LAPACK
+// error, 0 on success.
+int Engine::solve_projected_schur(int k, int nkeep, bool reorder, int *target_pos) {
+    auto t0 = std::chrono::steady_clock::now();
+    const int bk = k, ld = (int)maxsub, one = 1;
+    int info = 0;
+    zc *MA = ws->MA, *MB = ws->MB;
+    zc *T = ws->SA, *Q = ws->ZB;
+    for (int j = 0; j < k; ++j)
+        for (int i = 0; i < k; ++i) {
+            const size_t e = i + (size_t)j * maxsub;
+            hC[e] = nu0 * MA[e] + mu0 * MB[e];
+            T[e] = MB[e];
+        }
+    scipy_zgetrf_(&bk, &bk, hC.data(), &ld, ipiv.data(), &info);
+    if (info > 0) return 1;
+    if (info < 0) return -1;
+    scipy_zgetrs_("N", &bk, &bk, hC.data(), &ld, ipiv.data(), T, &ld, &info);
+    if (info) return -1;
+    const int lw = (int)zwork.size();
+    scipy_zgehrd_(&bk, &one, &bk, T, &ld, tau.data(), zwork.data(), &lw, &info);
+    if (info) return -1;
+    for (int j = 0; j < k; ++j) memcpy(Q + (size_t)j * maxsub, T + (size_t)j * maxsub, sizeof(zc) * k);
+    scipy_zunghr_(&bk, &one, &bk, Q, &ld, tau.data(), zwork.data(), &lw, &info);
+    if (info) return -1;
+    // the reflectors below the subdiagonal are not part of H
+    for (int j = 0; j < k; ++j)
+        for (int i = j + 2; i < k; ++i) T[i + (size_t)j * maxsub] = 0.0;
+    scipy_zhseqr_("S", "V", &bk, &one, &bk, T, &ld, omega.data(), Q, &ld, zwork.data(), &lw, &info);
+    if (info) return -1;
+    for (int j = 0; j < k; ++j)
+        for (int i = j + 1; i < k; ++i) T[i + (size_t)j * maxsub] = 0.0;
+    auto to_lambda = [&](int i) {
+        const zc w = omega[i];
+        if (std::abs(w) < 1e-300 * std::abs(nu0)) { alpha[i] = 1.0; beta[i] = 0.0; return; }
+        alpha[i] = (1.0 / w - mu0) / nu0;
+        beta[i] = 1.0;
+    };
+    for (int i = 0; i < k; ++i) to_lambda(i);
+    if (reorder) {
+        select_and_scan(k, nkeep, nullptr);
+        int m = 0;
+        double s = 0, sep = 0;
+        scipy_ztrsen_("N", "V", sel.data(), &bk, T, &ld, Q, &ld, omega.data(), &m, &s, &sep,
+                      zwork.data(), &lw, &info);
+        if (info) return -1;
+        for (int i = 0; i < k; ++i) to_lambda(i);
+    }
+    select_and_scan(k, 0, target_pos);
+    schur_step = true;
     qz_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     return 0;
+}
+
+// Ritz coefficients x = Z[:, 0:p+1] y of the target pair at position p
+// (reference jd_core.c:851-870): y solves the leading p x p triangular system
+// of (tb SA - ta SB) with y[p] = 1 (QZ form), or of (T - omega_p I) in the
+// harmonic Schur form.
+void Engine::ritz_coefficients(int k, int p, zc ta, zc tb, cplx *x) {
+    std::vector<zc> y(p + 1);
+    y[p] = 1.0;
+    const zc *SA = ws->SA, *SB = ws->SB, *ZB = ws->ZB;
+    const zc wp = schur_step ? SA[p + (size_t)p * maxsub] : zc(0.0);
+    for (int i = p - 1; i >= 0; --i) {
+        zc acc = 0.0, d;
+        if (schur_step) {
+            for (int j = i + 1; j <= p; ++j) acc += SA[i + (size_t)j * maxsub] * y[j];
+            d = SA[i + (size_t)i * maxsub] - wp;
+        } else {
+            for (int j = i + 1; j <= p; ++j)
+                acc += (tb * SA[i + (size_t)j * maxsub] - ta * SB[i + (size_t)j * maxsub]) * y[j];
+            d = tb * SA[i + (size_t)i * maxsub] - ta * SB[i + (size_t)i * maxsub];
+        }
+        y[i] = (std::abs(d) > 1e-300) ? -acc / d : zc(0.0);
+    }
+    for (int64_t i = 0; i < k; ++i) {
+        zc acc = 0.0;
+        for (int j = 0; j <= p; ++j) acc += ZB[i + (size_t)j * maxsub] * y[j];
+        x[i] = C(acc);
+    }
 }
 
 // Complex Givens with real cs >= 0 (reference jd_core.c:477-511).
@@ -410,7 +530,7 @@ bbjd_status Engine::gmres(int ndefl, zc ta, zc tb, const cplx *r, cplx *z) {
             if (pin_i[0]) h += Z(pin[kk + 1 + i]);
             H[i + (size_t)j * (ims + 1)] = h;
         }
-        if (pin_i[0]) dgks++;
+        if (pin_i[0]) { dgks++; second_pass_bytes(KC_GMRES, kk); }
         const double hjj1 = pin_d[0];
         H[(j + 1) + (size_t)j * (ims + 1)] = hjj1;
         if (hjj1 < 1e-14 * w_before) { j++; break; }               // jd_core.c:674
@@ -473,6 +593,14 @@ bbjd_status Engine::run() {
         nu0 = 1.0;
         mu0 = 0.0;
     }
+    {
+        const int want = ext ? ext->projected : BBJD_PROJ_QZ;
+        const bool harmonic = std::abs(nu0) > 0.0;
+        proj_mode = (want == BBJD_PROJ_QZ || !harmonic) ? BBJD_PROJ_QZ : BBJD_PROJ_SCHUR;
+        lock_rule = ext ? ext->lock_rule : BBJD_LOCK_ROBUST;
+        lock_rel = (ext && ext->lock_rel > 0) ? ext->lock_rel : 1e-6;
+        locks.clear();
+    }
     // start vector (jd_core.c:791-805): v0, else the C library's rand() seeded 42
     ws->kdim = 0;
     ws->nlock = 0;
@@ -523,31 +651,18 @@ bbjd_status Engine::run() {
         {
             int64_t nkeep = minsub - locked;                        // jd_core.c:830-831
             if (nkeep < 1) nkeep = 1;
-            if (solve_projected((int)k, (int)locked, (int)nkeep, &tpos)) {
+            int rc = 1;
+            if (proj_mode == BBJD_PROJ_SCHUR)
+                rc = solve_projected_schur((int)k, (int)nkeep, k >= maxsub, &tpos);
+            if (rc > 0) rc = solve_projected((int)k, (int)locked, (int)nkeep, &tpos);
+            if (rc) {
                 res->status = BBJD_ERR_LAPACK;
                 return res->status;
             }
         }
         // Ritz pair at the target position (jd_core.c:851-872)
         const zc ta = alpha[tpos], tb = beta[tpos];
-        {
-            const int p = tpos;
-            std::vector<zc> y(p + 1);
-            y[p] = 1.0;
-            const zc *SA = ws->SA, *SB = ws->SB, *ZB = ws->ZB;
-            for (int i = p - 1; i >= 0; --i) {
-                zc acc = 0.0;
-                for (int j = i + 1; j <= p; ++j)
-                    acc += (tb * SA[i + (size_t)j * maxsub] - ta * SB[i + (size_t)j * maxsub]) * y[j];
-                const zc d = tb * SA[i + (size_t)i * maxsub] - ta * SB[i + (size_t)i * maxsub];
-                y[i] = (std::abs(d) > 1e-300) ? -acc / d : zc(0.0);
-            }
-            for (int64_t i = 0; i < k; ++i) {
-                zc acc = 0.0;
-                for (int j = 0; j <= p; ++j) acc += ZB[i + (size_t)j * maxsub] * y[j];
-                pin[i] = C(acc);
-            }
-        }
+        ritz_coefficients((int)k, tpos, ta, tb, pin);
         BBJD_CUDA_TRY(cudaMemcpyAsync(xdev, pin, sizeof(cplx) * k, cudaMemcpyHostToDevice, st));
         // u = V x, ||u||, u /= ||u||  (jd_core.c:871-877)
         T.begin(KC_RITZ, 16.0 * n * (k + 1.0) + 32.0 * n);
@@ -579,6 +694,35 @@ bbjd_status Engine::run() {
         }
         if (rel < tol) {                                            // jd_core.c:905-932
             const zc lam = std::abs(tb) > 1e-300 ? ta / tb : ta;
+            if (lock_rule == BBJD_LOCK_ROBUST && ws->nlock > 0 && !locks.empty()) {
+                // is u (to 1e-8) inside the span of the locked Schur vectors,
+                // with a value close to a locked one?  Then it is a locked pair
+                // converging again: widen that pair's window, do not return it.
+                const int nl = (int)ws->nlock;
+                if ((s = tsdot(S, 1, 1, nl, ld, reinterpret_cast<cplx *>(ws->Q_right), nullptr, u,
+                               nullptr, S.red, nullptr, st)))
+                    return s;
+                BBJD_CUDA_TRY(cudaMemcpyAsync(pin, S.red, sizeof(cplx) * (nl + 1), cudaMemcpyDeviceToHost, st));
+                if ((s = sync())) return s;
+                double proj = 0.0;
+                for (int j = 0; j < nl; ++j) proj += pin[j].x * pin[j].x + pin[j].y * pin[j].y;
+                const double unrm2 = pin[nl].x > 0 ? pin[nl].x : 1.0;
+                size_t jbest = 0;
+                for (size_t j = 1; j < locks.size(); ++j)
+                    if (std::abs(lam - locks[j].value) < std::abs(lam - locks[jbest].value)) jbest = j;
+                const double drift = std::abs(lam - locks[jbest].value);
+                if (proj / unrm2 > 1.0 - 1e-8 && drift < 1e-4 * std::max(1.0, std::abs(lam))) {
+                    locks[jbest].window = std::max(locks[jbest].window, 10.0 * drift);
+                    duplicates++;
+                    if (P->verbose >= 1)
+                        fprintf(stderr, "  --- locked pair #%zu converged again (drift %.2e): window widened\n",
+                                jbest + 1, drift);
+                    continue;
+                }
+            }
+            locks.push_back({lam, lock_rule == BBJD_LOCK_ROBUST
+                                      ? std::max(tol * 100, lock_rel * std::max(1.0, std::abs(lam)))
+                                      : tol * 100});
             res->eigenvalues[res->nconv] = lam;
             BBJD_CUDA_TRY(cudaMemcpyAsync(res->eigenvectors + (size_t)res->nconv * n, u,
                                           sizeof(cplx) * n, cudaMemcpyDeviceToHost, st));
@@ -677,7 +821,7 @@ bbjd_status Engine::run() {
         BBJD_CUDA_TRY(cudaMemcpyAsync(pin_d + SC_VNORM, dscal + SC_VNORM, sizeof(double), cudaMemcpyDeviceToHost, st));
         BBJD_CUDA_TRY(cudaMemcpyAsync(pin_i + FL_T, dflag + FL_T, sizeof(int), cudaMemcpyDeviceToHost, st));
         if ((s = sync())) return s;
-        if (pin_i[FL_T]) dgks++;
+        if (pin_i[FL_T]) { dgks++; second_pass_bytes(KC_ORTH, (int)k); }
         if (pin_d[SC_VNORM] < 1e-14) {
             std::vector<zc> rv(n);
             for (int64_t i = 0; i < n; ++i) {
@@ -724,7 +868,7 @@ bbjd_status Engine::run() {
         BBJD_CUDA_TRY(cudaMemcpyAsync(pin_i + FL_W, dflag + FL_W, sizeof(int), cudaMemcpyDeviceToHost, st));
         BBJD_CUDA_TRY(cudaMemcpyAsync(pin, hAB, sizeof(cplx) * 2 * k, cudaMemcpyDeviceToHost, st));
         if ((s = sync())) return s;
-        if (pin_i[FL_W]) dgks++;
+        if (pin_i[FL_W]) { dgks++; second_pass_bytes(KC_PENCIL, (int)k); }
         if (pin_d[SC_WNORM] < 1e-14) {                              // jd_core.c:1061-1064
             BBJD_CUDA_TRY(cudaMemcpyAsync(wnew, AVk, sizeof(cplx) * n, cudaMemcpyDeviceToDevice, st));
             if ((s = orthogonalize(W, ld, (int)k, wnew, dscal + SC_WNORM, KC_PENCIL))) return s;

