@@ -107,6 +107,9 @@ SIGNATURES = {
                                     C.c_void_p, C.POINTER(Workspace), C.POINTER(Result)]),
     "bbjd_dev_orthogonalize": (C.c_int, [bbjd_int, bbjd_int, C.c_void_p, bbjd_int, C.c_void_p,
                                          C.POINTER(C.c_double), C.POINTER(C.c_int), C.c_void_p]),
+    "bbjd_dev_orthogonalize_static": (C.c_int, [bbjd_int, bbjd_int, C.c_void_p, bbjd_int,
+                                                C.c_void_p, C.POINTER(C.c_double),
+                                                C.POINTER(C.c_int), C.c_void_p]),
     "bbjd_dev_restart_gemm": (C.c_int, [bbjd_int, bbjd_int, bbjd_int, C.c_void_p, bbjd_int,
                                         C.c_void_p, bbjd_int, C.c_void_p, C.c_void_p]),
     "bbjd_dev_gram": (C.c_int, [bbjd_int, bbjd_int, C.c_void_p, C.c_void_p, bbjd_int,

@@ -424,6 +424,12 @@ bbjd_status tsdot(Scratch &S, int NM, int NV, int ncols, int64_t ld, const cplx 
     return BBJD_SUCCESS;
 }
 
+bbjd_status tsdot_allow_smem(size_t bytes) {
+    if (bytes <= 48 * 1024) return BBJD_SUCCESS;
+    BBJD_CUDA_TRY(cudaFuncSetAttribute(k_tsdot<1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    return BBJD_SUCCESS;
+}
+
 bbjd_status reduce_partials(const cplx *partial, int G, int X, cplx *out, cudaStream_t st) {
     k_reduce<<<(X + 31) / 32, 256, 0, st>>>(partial, G, X, out, nullptr);
     BBJD_LAUNCH_CHECK();

@@ -47,6 +47,9 @@ bbjd_status svdv(Scratch &S, const cplx *dots, const cplx *z, const cplx *s, cpl
                  cudaStream_t st);
 bbjd_status restart_gemm(int64_t n, int k, int keep, const cplx *X, int64_t ldx, const cplx *Z_dev,
                          int ldz, cplx *out, cudaStream_t st);
+// Raise the dynamic shared-memory limit of the one-matrix, one-vector dot
+// kernel to `bytes` (no-op up to 48 KB).
+bbjd_status tsdot_allow_smem(size_t bytes);
 // out[x] = sum_g partial[g*X + x], fixed order.
 bbjd_status reduce_partials(const cplx *partial, int G, int X, cplx *out, cudaStream_t st);
 // out (keep x keep col-major, device) = X^H Y; partial holds Gg*keep*keep.

@@ -132,6 +132,25 @@ bbjd_status bbjd_dev_orthogonalize(bbjd_int n, bbjd_int k, const bbjd_zomplex *Q
                                    bbjd_int ldq, bbjd_zomplex *v, double *norm_out,
                                    int *second_pass_out, void *stream);
 
+/* The same orthogonalisation as bbjd_dev_orthogonalize, allocating nothing
+ * (no counterpart in the reference).  For callers that cannot call
+ * cudaMalloc there: a framework that owns all device memory and forbids
+ * allocation after start-up, or a pipeline that must not stall the device
+ * (cudaMalloc and cudaFree synchronise it).  Its reduction scratch is one
+ * static device array of about 2.7 MB in the library, held by every GPU
+ * that loads the library until exit.  Limits: n <= BBJD_STATIC_ORTH_MAX_N,
+ * k <= BBJD_STATIC_ORTH_MAX_K; larger sizes return BBJD_ERR_INVALID with a
+ * message on stderr.  The first call on each device looks the array up
+ * (cudaGetSymbolAddress).  Calls share the array: two calls that overlap on
+ * the GPU (other streams or host threads on the same device) race, so
+ * serialise them.  Q and v are device pointers; *norm_out and
+ * *second_pass_out are host. */
+#define BBJD_STATIC_ORTH_MAX_N 8388608
+#define BBJD_STATIC_ORTH_MAX_K 256
+bbjd_status bbjd_dev_orthogonalize_static(bbjd_int n, bbjd_int k, const bbjd_zomplex *Q,
+                                          bbjd_int ldq, bbjd_zomplex *v, double *norm_out,
+                                          int *second_pass_out, void *stream);
+
 /* out = X[:, 0:k] * Z[0:k, 0:keep]  (X, out ld = ldx; Z host k x keep col-major,
  * ldz).  Thick-restart compression, reference jd_core.c:989-999. */
 bbjd_status bbjd_dev_restart_gemm(bbjd_int n, bbjd_int k, bbjd_int keep,
