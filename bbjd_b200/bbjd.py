@@ -233,7 +233,7 @@ _LOCK = {"robust": 0, "reference": 1}
 
 def _solve_device(dev: DevicePencil, pc, k, sigma, target, tol, maxiter, maxsub, minsub,
                   inner_maxiter, inner_tol, v0, verbose, timing, projected="auto",
-                  lock="robust"):
+                  lock="robust", precision="fp64"):
     lib = _lib.load()
     n = dev.n
     p = _lib.Params()
@@ -249,6 +249,9 @@ def _solve_device(dev: DevicePencil, pc, k, sigma, target, tol, maxiter, maxsub,
     ext = _lib.DeviceExt()
     lib.bbjd_device_ext_init(C.byref(ext))
     ext.record_timing = 1 if timing else 0
+    if precision not in ("fp64", "mixed"):
+        raise ValueError("precision must be 'fp64' or 'mixed'")
+    ext.precision = 1 if precision == "mixed" else 0
     if projected not in _PROJECTED:
         raise ValueError(f"projected must be one of {list(_PROJECTED)}")
     ext.projected = _PROJECTED[projected]
@@ -300,6 +303,7 @@ def jdqz(
     timing: bool = False,
     projected: str = "auto",
     lock: str = "robust",
+    precision: str = "fp64",
 ):
     """Jacobi-Davidson QZ for ``A x = lambda B x``, the eigenvalues nearest
     ``sigma`` first.  Parameters, defaults, returns and errors are those of
@@ -320,7 +324,10 @@ def jdqz(
     ``lock`` picks how converged values are recognised: 'robust' (a relative
     window and an eigenvector-angle test, so an ill-conditioned eigenvalue is
     not returned twice) or 'reference' (the reference's absolute 100 tol
-    window, jd_core.c:369, 439).
+    window, jd_core.c:369, 439).  ``precision='mixed'`` stores the device
+    LU factors in complex64 and runs the first CGS pass against V over a
+    complex64 copy of V (the second pass, DGKS, residuals, projected pencil
+    and QZ stay FP64).
     """
     if which not in _TARGET_MAP:
         raise ValueError(f"which must be one of {list(_TARGET_MAP.keys())}; got {which!r}")
@@ -342,7 +349,7 @@ def jdqz(
         elif isinstance(preconditioner, DevicePreconditioner):
             pc = preconditioner
         elif isinstance(preconditioner, str):
-            pc = DevicePreconditioner(dev, sigma, preconditioner)
+            pc = DevicePreconditioner(dev, sigma, preconditioner, precision=precision)
             own_pc = True
         else:
             raise ValueError("with a block-bordered pencil the preconditioner must be 'exact', "
@@ -350,7 +357,7 @@ def jdqz(
         try:
             ev, evecs, resid, nconv, iters, status, stats = _solve_device(
                 dev, pc, k, sigma, target, tol, maxiter, maxsub, minsub, inner_maxiter,
-                inner_tol, v0, verbose, timing, projected, lock)
+                inner_tol, v0, verbose, timing, projected, lock, precision)
         finally:
             if own_pc:
                 pc.close()

@@ -7,6 +7,20 @@
 
 struct bbjd_precond;
 
+namespace bbjd {
+// Reduction scratch of one fused product (tau-row partials and the residual
+// norm).  The matrix owns one; each device solve owns another, so solves on
+// different streams never share it.
+struct BBTScratch {
+    int G = 0;                       // CTAs of the product kernel
+    cplx *tau_part = nullptr;        // [G][t]
+    double *rn_part = nullptr;       // [G]
+    double *rnorm = nullptr;         // ||r|| of the last residual product
+    double *rtau_nsq = nullptr;      // [t] |r|^2 of the tau rows
+    unsigned *counter = nullptr;     // completion counter of the norm reduction
+};
+}  // namespace bbjd
+
 struct bbjd_bbt_matrix {
     int b = 0, t = 0;
     int64_t nblk = 0, nb = 0, n = 0;
@@ -14,21 +28,19 @@ struct bbjd_bbt_matrix {
     bbjd::cplx *E = nullptr;   // nb x t col-major
     bbjd::cplx *FT = nullptr;  // n x t row-major == F (t x n) col-major
     bbjd::cplx *mem = nullptr;
-    // scratch of the fused product
-    int G = 0;
-    bbjd::cplx *tau_part = nullptr;  // [G][t]
-    double *rn_part = nullptr;       // [G]
-    double *rnorm = nullptr;         // device scalar: ||r|| of the last residual product
+    bbjd::BBTScratch sc;             // scratch of bbjd_bbt_matvec
 };
 
 namespace bbjd {
 
 // yA = A x, yB = B x; if r != nullptr also r = tb*yA - ta*yB and
-// *rnorm = ||r|| (device; m->rnorm when null).  One pass over the pencil's
-// storage.  The product's scratch lives in the matrix: one product at a time
-// per matrix.
-bbjd_status bbt_apply(const bbjd_bbt_matrix *m, const cplx *x, cplx *yA, cplx *yB, cplx ta,
-                      cplx tb, cplx *r, double *rnorm, cudaStream_t st);
+// *rnorm = ||r|| (device; sc->rnorm when null).  One pass over the pencil's
+// storage, with the caller's scratch (the matrix's own when sc is null; two
+// products in flight at once need two scratches).
+bbjd_status bbt_apply(const bbjd_bbt_matrix *m, const BBTScratch *sc, const cplx *x, cplx *yA,
+                      cplx *yB, cplx ta, cplx tb, cplx *r, double *rnorm, cudaStream_t st);
+bbjd_status bbt_scratch_alloc(const bbjd_bbt_matrix *m, BBTScratch *sc);
+void bbt_scratch_free(BBTScratch *sc);
 bbjd_status precond_solve(const bbjd_precond *pc, int nrhs, const cplx *r, cplx *x, int64_t stride,
                           cudaStream_t st);
 double precond_bytes(const bbjd_precond *pc, int nrhs);
@@ -50,7 +62,11 @@ struct bbjd_precond {
     };
     std::vector<Level> levels;
     bbjd::cplx *Dinv_top = nullptr;
-    bbjd::cplx *pool = nullptr;     // all factor blocks
+    bbjd::cplx *pool = nullptr;     // all factor blocks (FP64; released in mixed precision)
+    const bbjd::cplx *pool_base = nullptr;  // the FP64 pool's address: offsets into pool32
+    int64_t pool_elems = 0;
+    float2 *pool32 = nullptr;       // complex64 copy of the factor blocks (mixed precision)
+    float2 *Y32 = nullptr, *FT32 = nullptr;
     // border (t > 0): Y = K^-1 E (nb x t col-major), Sinv = (G - F1 Y)^-1 (t x t)
     bbjd::cplx *Y = nullptr;
     bbjd::cplx *Sinv = nullptr;
@@ -64,6 +80,7 @@ struct bbjd_precond {
     int G = 0;
     bbjd::cplx *tau_part = nullptr;  // [G][2][t]
     bbjd::cplx *x2 = nullptr;        // [2][t]
+    bbjd::cplx *gbuf = nullptr;      // [2][t] r2 - F1 y
     int *err = nullptr;              // device: singular pivot seen
     double factor_seconds = 0.0;
     double min_pivot = 0.0;

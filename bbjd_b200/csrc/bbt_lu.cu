@@ -22,12 +22,28 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <mutex>
+#include <type_traits>
 #include <vector>
 
 extern "C" void scipy_zgesv_(const int *n, const int *nrhs, bbjd_zomplex *a, const int *lda,
                              int *ipiv, bbjd_zomplex *b, const int *ldb, int *info);
 
 namespace bbjd {
+
+// Factor loads: FP64 blocks, or complex64 blocks (the mixed-precision form)
+// widened to FP64 for the arithmetic.
+__device__ __forceinline__ cplx ldm(const double2 *p) { return __ldcs(p); }
+__device__ __forceinline__ cplx ldm(const float2 *p) {
+    const float2 f = __ldcs(p);
+    return mk((double)f.x, (double)f.y);
+}
+
+__global__ void k_to_c64(int64_t count, const double2 *__restrict__ in, float2 *__restrict__ out) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += stride)
+        out[i] = make_float2((float)in[i].x, (float)in[i].y);
+}
 
 // ---------------------------------------------------------------------------
 // Shared-memory block helpers (row-major, padded row stride).
@@ -275,12 +291,12 @@ __global__ void __launch_bounds__(256) k_bcr_even(
 // ---------------------------------------------------------------------------
 // Solve kernels: a warp owns 32/BS blocks; lane = row; R right-hand sides
 // stored with a stride.  y_row += M v with v spread over the block's lanes.
-template <int BS, int R>
-__device__ __forceinline__ void bmv_add(cplx (&acc)[R], const cplx *__restrict__ Mb, int row,
+template <int BS, int R, typename T>
+__device__ __forceinline__ void bmv_add(cplx (&acc)[R], const T *__restrict__ Mb, int row,
                                         const cplx (&v)[R], int base, double sign) {
 #pragma unroll 8
     for (int c = 0; c < BS; ++c) {
-        const cplx mv = ldg_stream(Mb + c * BS + row);
+        const cplx mv = ldm(Mb + c * BS + row);
 #pragma unroll
         for (int q = 0; q < R; ++q) {
             const cplx vc = shfl(v[q], base + c);
@@ -291,9 +307,9 @@ __device__ __forceinline__ void bmv_add(cplx (&acc)[R], const cplx *__restrict__
 }
 
 // rhs_next[m/2] = rhs[m] - Alpha rhs[m-1] - Beta rhs[m+1] for even m.
-template <int BS, int R>
-__global__ void __launch_bounds__(256) k_bcr_fwd(int64_t N, const cplx *__restrict__ Alpha,
-                                                 const cplx *__restrict__ Beta,
+template <int BS, int R, typename T>
+__global__ void __launch_bounds__(256) k_bcr_fwd(int64_t N, const T *__restrict__ Alpha,
+                                                 const T *__restrict__ Beta,
                                                  const cplx *__restrict__ rhs, int64_t rs,
                                                  cplx *__restrict__ nxt, int64_t ns) {
     constexpr int BPW = 32 / BS, BB = BS * BS;
@@ -313,8 +329,8 @@ __global__ void __launch_bounds__(256) k_bcr_fwd(int64_t N, const cplx *__restri
             vp[q] = m >= 1 ? rhs[q * rs + (m - 1) * BS + row] : mk(0.0, 0.0);
             vn[q] = m + 1 < N ? rhs[q * rs + (m + 1) * BS + row] : mk(0.0, 0.0);
         }
-        bmv_add<BS, R>(acc, Alpha + ic * BB, row, vp, base, -1.0);
-        bmv_add<BS, R>(acc, Beta + ic * BB, row, vn, base, -1.0);
+        bmv_add<BS, R, T>(acc, Alpha + ic * BB, row, vp, base, -1.0);
+        bmv_add<BS, R, T>(acc, Beta + ic * BB, row, vn, base, -1.0);
         if (valid)
 #pragma unroll
             for (int q = 0; q < R; ++q) nxt[q * ns + i * BS + row] = acc[q];
@@ -322,8 +338,8 @@ __global__ void __launch_bounds__(256) k_bcr_fwd(int64_t N, const cplx *__restri
 }
 
 // x = Dinv rhs for a single block (top of the reduction).
-template <int BS, int R>
-__global__ void k_bcr_top(const cplx *__restrict__ Dinv, const cplx *__restrict__ rhs, int64_t rs,
+template <int BS, int R, typename T>
+__global__ void k_bcr_top(const T *__restrict__ Dinv, const cplx *__restrict__ rhs, int64_t rs,
                           cplx *__restrict__ x, int64_t xs) {
     const int lane = threadIdx.x & 31, row = lane % BS, base = 0;
     const bool active = lane < BS;
@@ -333,7 +349,7 @@ __global__ void k_bcr_top(const cplx *__restrict__ Dinv, const cplx *__restrict_
         acc[q] = mk(0.0, 0.0);
         v[q] = active ? rhs[q * rs + row] : mk(0.0, 0.0);
     }
-    bmv_add<BS, R>(acc, Dinv, row, v, base, 1.0);
+    bmv_add<BS, R, T>(acc, Dinv, row, v, base, 1.0);
     if (active)
 #pragma unroll
         for (int q = 0; q < R; ++q) x[q * xs + row] = acc[q];
@@ -341,10 +357,10 @@ __global__ void k_bcr_top(const cplx *__restrict__ Dinv, const cplx *__restrict_
 
 // Back substitution of one level: even m copy from the level above,
 // odd m: x = Dinv rhs - DinvLo x[m-1] - DinvUp x[m+1].
-template <int BS, int R>
-__global__ void __launch_bounds__(256) k_bcr_bwd(int64_t N, const cplx *__restrict__ Dinv,
-                                                 const cplx *__restrict__ DinvLo,
-                                                 const cplx *__restrict__ DinvUp,
+template <int BS, int R, typename T>
+__global__ void __launch_bounds__(256) k_bcr_bwd(int64_t N, const T *__restrict__ Dinv,
+                                                 const T *__restrict__ DinvLo,
+                                                 const T *__restrict__ DinvUp,
                                                  const cplx *__restrict__ rhs, int64_t rs,
                                                  const cplx *__restrict__ xup, int64_t us,
                                                  cplx *__restrict__ x, int64_t xs) {
@@ -373,18 +389,117 @@ __global__ void __launch_bounds__(256) k_bcr_bwd(int64_t N, const cplx *__restri
             vp[q] = xup[q * us + ic * BS + row];                                  // x[m-1]
             vn[q] = m + 1 < N ? xup[q * us + (ic + 1) * BS + row] : mk(0.0, 0.0);  // x[m+1]
         }
-        bmv_add<BS, R>(acc, Dinv + ic * BB, row, r, base, 1.0);
-        bmv_add<BS, R>(acc, DinvLo + ic * BB, row, vp, base, -1.0);
-        bmv_add<BS, R>(acc, DinvUp + ic * BB, row, vn, base, -1.0);
+        bmv_add<BS, R, T>(acc, Dinv + ic * BB, row, r, base, 1.0);
+        bmv_add<BS, R, T>(acc, DinvLo + ic * BB, row, vp, base, -1.0);
+        bmv_add<BS, R, T>(acc, DinvUp + ic * BB, row, vn, base, -1.0);
         if (valid)
 #pragma unroll
             for (int q = 0; q < R; ++q) x[q * xs + m * BS + row] = acc[q];
     }
 }
 
+// Small levels: one CTA per block.  The BS columns of each b x b block are
+// split over NS = 256/BS column slots (slot = 8 warps x 32/BS lane groups),
+// so each thread's chain of dependent loads is BS^2/256 columns long instead
+// of BS; the slots' partial sums meet in shared memory.  Used when a level
+// has too few blocks to fill the GPU with one warp per block.
+template <int BS, int R, typename T>
+__device__ __forceinline__ void slot_mv(cplx (&acc)[R], const T *__restrict__ Mb, int row, int c0,
+                                        int nc, const cplx (&v)[R], int base, double sign) {
+    for (int c = c0; c < c0 + nc; ++c) {
+        const cplx mv = ldm(Mb + c * BS + row);
+#pragma unroll
+        for (int q = 0; q < R; ++q) {
+            const cplx vc = shfl(v[q], base + c);
+            if (sign > 0) cfma(acc[q], mv, vc);
+            else cfms(acc[q], mv, vc);
+        }
+    }
+}
+
+template <int BS, int R, typename T>
+__global__ void __launch_bounds__(256) k_bcr_fwd_cta(int64_t N, const T *__restrict__ Alpha,
+                                                     const T *__restrict__ Beta,
+                                                     const cplx *__restrict__ rhs, int64_t rs,
+                                                     cplx *__restrict__ nxt, int64_t ns) {
+    constexpr int BB = BS * BS, GPW = 32 / BS, NS = 8 * GPW, CPS = BS / NS;
+    __shared__ cplx red[NS][R][BS];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int grp = lane / BS, row = lane - grp * BS, base = grp * BS;
+    const int slot = warp * GPW + grp, c0 = slot * CPS;
+    const int64_t neven = (N + 1) / 2;
+    for (int64_t i = blockIdx.x; i < neven; i += gridDim.x) {
+        const int64_t m = 2 * i;
+        cplx acc[R], vp[R], vn[R];
+#pragma unroll
+        for (int q = 0; q < R; ++q) {
+            acc[q] = mk(0.0, 0.0);
+            vp[q] = m >= 1 ? rhs[q * rs + (m - 1) * BS + row] : mk(0.0, 0.0);
+            vn[q] = m + 1 < N ? rhs[q * rs + (m + 1) * BS + row] : mk(0.0, 0.0);
+        }
+        slot_mv<BS, R, T>(acc, Alpha + i * BB, row, c0, CPS, vp, base, -1.0);
+        slot_mv<BS, R, T>(acc, Beta + i * BB, row, c0, CPS, vn, base, -1.0);
+#pragma unroll
+        for (int q = 0; q < R; ++q) red[slot][q][row] = acc[q];
+        __syncthreads();
+        for (int e = threadIdx.x; e < R * BS; e += blockDim.x) {
+            const int q = e / BS, rr = e - q * BS;
+            cplx s = rhs[q * rs + m * BS + rr];
+            for (int k = 0; k < NS; ++k) s = cadd(s, red[k][q][rr]);
+            nxt[q * ns + i * BS + rr] = s;
+        }
+        __syncthreads();
+    }
+}
+
+template <int BS, int R, typename T>
+__global__ void __launch_bounds__(256) k_bcr_bwd_cta(int64_t N, const T *__restrict__ Dinv,
+                                                     const T *__restrict__ DinvLo,
+                                                     const T *__restrict__ DinvUp,
+                                                     const cplx *__restrict__ rhs, int64_t rs,
+                                                     const cplx *__restrict__ xup, int64_t us,
+                                                     cplx *__restrict__ x, int64_t xs) {
+    constexpr int BB = BS * BS, GPW = 32 / BS, NS = 8 * GPW, CPS = BS / NS;
+    __shared__ cplx red[NS][R][BS];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int grp = lane / BS, row = lane - grp * BS, base = grp * BS;
+    const int slot = warp * GPW + grp, c0 = slot * CPS;
+    const int64_t nodd = N / 2, neven = (N + 1) / 2;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < neven * BS;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t ie = e / BS, rr = e - ie * BS;
+#pragma unroll
+        for (int q = 0; q < R; ++q) x[q * xs + (2 * ie) * BS + rr] = xup[q * us + ie * BS + rr];
+    }
+    for (int64_t i = blockIdx.x; i < nodd; i += gridDim.x) {
+        const int64_t m = 2 * i + 1;
+        cplx acc[R], r[R], vp[R], vn[R];
+#pragma unroll
+        for (int q = 0; q < R; ++q) {
+            acc[q] = mk(0.0, 0.0);
+            r[q] = rhs[q * rs + m * BS + row];
+            vp[q] = xup[q * us + i * BS + row];
+            vn[q] = m + 1 < N ? xup[q * us + (i + 1) * BS + row] : mk(0.0, 0.0);
+        }
+        slot_mv<BS, R, T>(acc, Dinv + i * BB, row, c0, CPS, r, base, 1.0);
+        slot_mv<BS, R, T>(acc, DinvLo + i * BB, row, c0, CPS, vp, base, -1.0);
+        slot_mv<BS, R, T>(acc, DinvUp + i * BB, row, c0, CPS, vn, base, -1.0);
+#pragma unroll
+        for (int q = 0; q < R; ++q) red[slot][q][row] = acc[q];
+        __syncthreads();
+        for (int e = threadIdx.x; e < R * BS; e += blockDim.x) {
+            const int q = e / BS, rr = e - q * BS;
+            cplx s = red[0][q][rr];
+            for (int k = 1; k < NS; ++k) s = cadd(s, red[k][q][rr]);
+            x[q * xs + m * BS + rr] = s;
+        }
+        __syncthreads();
+    }
+}
+
 // Block-Jacobi apply: x_j = Dinv_j r_j for every interior block.
-template <int BS, int R>
-__global__ void __launch_bounds__(256) k_bjac(int64_t nblk, const cplx *__restrict__ Dinv,
+template <int BS, int R, typename T>
+__global__ void __launch_bounds__(256) k_bjac(int64_t nblk, const T *__restrict__ Dinv,
                                               const cplx *__restrict__ r, int64_t rs,
                                               cplx *__restrict__ x, int64_t xs) {
     constexpr int BPW = 32 / BS, BB = BS * BS;
@@ -401,26 +516,26 @@ __global__ void __launch_bounds__(256) k_bjac(int64_t nblk, const cplx *__restri
             acc[q] = mk(0.0, 0.0);
             v[q] = r[q * rs + jc * BS + row];
         }
-        bmv_add<BS, R>(acc, Dinv + jc * BB, row, v, base, 1.0);
+        bmv_add<BS, R, T>(acc, Dinv + jc * BB, row, v, base, 1.0);
         if (valid)
 #pragma unroll
             for (int q = 0; q < R; ++q) x[q * xs + j * BS + row] = acc[q];
     }
 }
 
-// Border step 1: per-CTA partials of F1 y (t-vector per RHS).
-template <int R>
-__global__ void __launch_bounds__(256) k_border_g(int64_t nb, int t, const cplx *__restrict__ FT,
+// Border step 1: per-CTA partials of F1 y (t-vector per RHS); lane owns tau
+// rows lane + 32 u (u < NQ).
+template <int R, int NQ, typename T>
+__global__ void __launch_bounds__(256) k_border_g(int64_t nb, int t, const T *__restrict__ FT,
                                                   const cplx *__restrict__ y, int64_t ys,
                                                   cplx *__restrict__ part) {
     extern __shared__ cplx wsm[];  // 8 warps x R x t
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int nq = (t + 31) / 32;
-    cplx acc[R][4];
+    cplx acc[R][NQ];
 #pragma unroll
     for (int q = 0; q < R; ++q)
 #pragma unroll
-        for (int u = 0; u < 4; ++u) acc[q][u] = mk(0.0, 0.0);
+        for (int u = 0; u < NQ; ++u) acc[q][u] = mk(0.0, 0.0);
     const int64_t ngroups = (nb + 31) / 32;
     const int64_t gw = (int64_t)blockIdx.x * 8 + warp, nw = (int64_t)gridDim.x * 8;
     for (int64_t g = gw; g < ngroups; g += nw) {
@@ -428,16 +543,17 @@ __global__ void __launch_bounds__(256) k_border_g(int64_t nb, int t, const cplx 
         cplx yv[R];
 #pragma unroll
         for (int q = 0; q < R; ++q) yv[q] = col < nb ? y[q * ys + col] : mk(0.0, 0.0);
+#pragma unroll 8
         for (int c = 0; c < 32; ++c) {
             const int64_t cc = min(g * 32 + c, nb - 1);
             cplx yc[R];
 #pragma unroll
             for (int q = 0; q < R; ++q) yc[q] = shfl(yv[q], c);
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
+            for (int u = 0; u < NQ; ++u) {
                 const int tau = lane + 32 * u;
-                if (u < nq && tau < t) {
-                    const cplx f = ldg_stream(FT + cc * t + tau);
+                if (tau < t) {
+                    const cplx f = ldm(FT + cc * t + tau);
 #pragma unroll
                     for (int q = 0; q < R; ++q) cfma(acc[q][u], f, yc[q]);
                 }
@@ -447,9 +563,9 @@ __global__ void __launch_bounds__(256) k_border_g(int64_t nb, int t, const cplx 
 #pragma unroll
     for (int q = 0; q < R; ++q)
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
+        for (int u = 0; u < NQ; ++u) {
             const int tau = lane + 32 * u;
-            if (u < nq && tau < t) wsm[(warp * R + q) * t + tau] = acc[q][u];
+            if (tau < t) wsm[(warp * R + q) * t + tau] = acc[q][u];
         }
     __syncthreads();
     for (int e = threadIdx.x; e < R * t; e += blockDim.x) {
@@ -460,34 +576,44 @@ __global__ void __launch_bounds__(256) k_border_g(int64_t nb, int t, const cplx 
     }
 }
 
-// Border step 2: x2 = Sinv (r2 - sum_g part); written to out[nb:] and x2buf.
+// Border step 2a: g[q][tau] = r2[q][tau] - sum_g part[g][q][tau], one warp
+// per (q, tau), lanes over the CTA partials (fixed order).
 template <int R>
-__global__ void __launch_bounds__(256) k_border_x2(int64_t nb, int t, int G,
-                                                   const cplx *__restrict__ part,
+__global__ void __launch_bounds__(256) k_border_gsum(int64_t nb, int t, int G,
+                                                     const cplx *__restrict__ part,
+                                                     const cplx *__restrict__ rin, int64_t rs,
+                                                     cplx *__restrict__ gbuf) {
+    const int w = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    if (w >= R * t) return;
+    const int q = w / t, tau = w - q * t;
+    cplx s = mk(0.0, 0.0);
+    for (int k = lane; k < G; k += 32) s = cadd(s, part[((int64_t)k * R + q) * t + tau]);
+    s = warp_sum(s);
+    if (lane == 0) gbuf[q * t + tau] = csub(rin[q * rs + nb + tau], s);
+}
+
+// Border step 2b: x2 = Sinv g; written to out[nb:] and x2buf.
+template <int R>
+__global__ void __launch_bounds__(256) k_border_x2(int64_t nb, int t, const cplx *__restrict__ gbuf,
                                                    const cplx *__restrict__ Sinv,
-                                                   const cplx *__restrict__ rin, int64_t rs,
                                                    cplx *__restrict__ out, int64_t os,
                                                    cplx *__restrict__ x2buf) {
     __shared__ cplx g[R][128];
-    for (int e = threadIdx.x; e < R * t; e += blockDim.x) {
-        const int q = e / t, tau = e - q * t;
-        cplx s = mk(0.0, 0.0);
-        for (int k = 0; k < G; ++k) s = cadd(s, part[((int64_t)k * R + q) * t + tau]);
-        g[q][tau] = csub(rin[q * rs + nb + tau], s);
-    }
+    for (int e = threadIdx.x; e < R * t; e += blockDim.x) g[e / t][e % t] = gbuf[e];
     __syncthreads();
-    for (int e = threadIdx.x; e < R * t; e += blockDim.x) {
-        const int q = e / t, tau = e - q * t;
-        cplx acc = mk(0.0, 0.0);
-        for (int c = 0; c < t; ++c) cfma(acc, Sinv[(int64_t)c * t + tau], g[q][c]);
-        out[q * os + nb + tau] = acc;
-        x2buf[q * t + tau] = acc;
-    }
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= R * t) return;
+    const int q = e / t, tau = e - q * t;
+    cplx acc = mk(0.0, 0.0);
+#pragma unroll 8
+    for (int c = 0; c < t; ++c) cfma(acc, Sinv[(int64_t)c * t + tau], g[q][c]);
+    out[q * os + nb + tau] = acc;
+    x2buf[q * t + tau] = acc;
 }
 
 // Border step 3: x1 = y - Y x2 (in place in out[0:nb]).
-template <int R>
-__global__ void __launch_bounds__(256) k_border_x1(int64_t nb, int t, const cplx *__restrict__ Y,
+template <int R, typename T>
+__global__ void __launch_bounds__(256) k_border_x1(int64_t nb, int t, const T *__restrict__ Y,
                                                    const cplx *__restrict__ x2buf,
                                                    cplx *__restrict__ out, int64_t os) {
     __shared__ cplx xs[R][128];
@@ -500,7 +626,7 @@ __global__ void __launch_bounds__(256) k_border_x1(int64_t nb, int t, const cplx
         for (int q = 0; q < R; ++q) acc[q] = out[q * os + i];
 #pragma unroll 8
         for (int tau = 0; tau < t; ++tau) {
-            const cplx yv = ldg_stream(Y + (int64_t)tau * nb + i);
+            const cplx yv = ldm(Y + (int64_t)tau * nb + i);
 #pragma unroll
             for (int q = 0; q < R; ++q) cfms(acc[q], yv, xs[q][tau]);
         }
@@ -575,6 +701,37 @@ static bbjd_status set_attrs() {
     return BBJD_SUCCESS;
 }
 
+// Levels with at most this many blocks to process run one CTA per block.
+constexpr int64_t kSmallLevel = 2048;
+
+static unsigned grid_for(int64_t items, int per_cta, int cap);
+
+// CTA-per-block launches exist for b >= 16 (b = 8 blocks are too small to split).
+template <int BS, int R, typename T>
+static bool fwd_cta(int64_t N, int64_t items, const T *Alpha, const T *Beta, const cplx *rhs,
+                    int64_t rs, cplx *nxt, int64_t ns, int cap, cudaStream_t st) {
+    if constexpr (BS >= 16) {
+        if (items > kSmallLevel) return false;
+        k_bcr_fwd_cta<BS, R, T><<<grid_for(items, 1, cap), 256, 0, st>>>(N, Alpha, Beta, rhs, rs, nxt, ns);
+        return true;
+    } else {
+        return false;
+    }
+}
+template <int BS, int R, typename T>
+static bool bwd_cta(int64_t N, int64_t items, const T *Dinv, const T *DinvLo, const T *DinvUp,
+                    const cplx *rhs, int64_t rs, const cplx *xup, int64_t us, cplx *x, int64_t xs,
+                    int cap, cudaStream_t st) {
+    if constexpr (BS >= 16) {
+        if (items > kSmallLevel) return false;
+        k_bcr_bwd_cta<BS, R, T><<<grid_for(std::max<int64_t>(items, 1), 1, cap), 256, 0, st>>>(
+            N, Dinv, DinvLo, DinvUp, rhs, rs, xup, us, x, xs);
+        return true;
+    } else {
+        return false;
+    }
+}
+
 static unsigned grid_for(int64_t items, int per_cta, int cap) {
     int64_t g = (items + per_cta - 1) / per_cta;
     if (g < 1) g = 1;
@@ -582,9 +739,19 @@ static unsigned grid_for(int64_t items, int per_cta, int cap) {
     return (unsigned)g;
 }
 
+// Factor array of type T: the FP64 pool, or its complex64 copy at the same
+// element offset (mixed precision; the FP64 pool is released after the copy).
+template <typename T>
+static const T *fac(const bbjd_precond *pc, const cplx *p64) {
+    if constexpr (std::is_same<T, float2>::value)
+        return pc->pool32 + (p64 - pc->pool_base);
+    else
+        return p64;
+}
+
 // Solve K x = r for the interior with R right-hand sides (input stride rs,
-// output stride xs).  x may alias r.
-template <int BS, int R>
+// output stride xs).  x may alias r.  T: factor element type.
+template <int BS, int R, typename T = cplx>
 static bbjd_status bcr_solve(const bbjd_precond *pc, const cplx *r, int64_t rs, cplx *x, int64_t xs,
                              cudaStream_t st) {
     // Vectors: level 0 is the caller's r / x; level l >= 1 and the top block
@@ -600,37 +767,46 @@ static bbjd_status bcr_solve(const bbjd_precond *pc, const cplx *r, int64_t rs, 
     for (int64_t l = 0; l < L; ++l) {
         const auto &lv = pc->levels[l];
         cplx *nxt = (l + 1 < L) ? pc->lvl_rhs + pc->levels[l + 1].vec_off : pc->lvl_rhs + pc->top_off;
-        const int64_t items = (lv.n_even + (32 / BS) - 1) / (32 / BS);
-        k_bcr_fwd<BS, R><<<grid_for(items, 8, cap), 256, 0, st>>>(lv.N, lv.Alpha, lv.Beta, rhs_at(l),
-                                                                 rstride(l), nxt, tot);
+        const T *Alpha = fac<T>(pc, lv.Alpha), *Beta = fac<T>(pc, lv.Beta);
+        if (!fwd_cta<BS, R, T>(lv.N, lv.n_even, Alpha, Beta, rhs_at(l), rstride(l), nxt, tot, cap, st)) {
+            const int64_t items = (lv.n_even + (32 / BS) - 1) / (32 / BS);
+            k_bcr_fwd<BS, R, T><<<grid_for(items, 8, cap), 256, 0, st>>>(lv.N, Alpha, Beta, rhs_at(l),
+                                                                        rstride(l), nxt, tot);
+        }
         BBJD_LAUNCH_CHECK();
     }
     cplx *tx = L ? pc->lvl_x + pc->top_off : x;
     const int64_t txs = L ? tot : xs;
-    k_bcr_top<BS, R><<<1, 32, 0, st>>>(pc->Dinv_top, rhs_at(L), rstride(L), tx, txs);
+    k_bcr_top<BS, R, T><<<1, 32, 0, st>>>(fac<T>(pc, pc->Dinv_top), rhs_at(L), rstride(L), tx, txs);
     BBJD_LAUNCH_CHECK();
     for (int64_t l = L - 1; l >= 0; --l) {
         const auto &lv = pc->levels[l];
         const cplx *xup = (l + 1 < L) ? pc->lvl_x + pc->levels[l + 1].vec_off : pc->lvl_x + pc->top_off;
         cplx *xo = l == 0 ? x : pc->lvl_x + lv.vec_off;
         const int64_t xos = l == 0 ? xs : tot;
-        const int64_t items = std::max<int64_t>((lv.n_odd + (32 / BS) - 1) / (32 / BS),
-                                                (lv.n_even * BS + 255) / 256);
-        k_bcr_bwd<BS, R><<<grid_for(items, 8, cap), 256, 0, st>>>(lv.N, lv.Dinv, lv.DinvLo, lv.DinvUp,
-                                                                 rhs_at(l), rstride(l), xup, tot,
-                                                                 xo, xos);
+        const T *Dinv = fac<T>(pc, lv.Dinv), *DinvLo = fac<T>(pc, lv.DinvLo);
+        const T *DinvUp = fac<T>(pc, lv.DinvUp);
+        if (!bwd_cta<BS, R, T>(lv.N, lv.n_odd, Dinv, DinvLo, DinvUp, rhs_at(l), rstride(l), xup, tot, xo,
+                               xos, cap, st)) {
+            const int64_t items = std::max<int64_t>((lv.n_odd + (32 / BS) - 1) / (32 / BS),
+                                                    (lv.n_even * BS + 255) / 256);
+            k_bcr_bwd<BS, R, T><<<grid_for(items, 8, cap), 256, 0, st>>>(lv.N, Dinv, DinvLo, DinvUp,
+                                                                        rhs_at(l), rstride(l), xup, tot,
+                                                                        xo, xos);
+        }
         BBJD_LAUNCH_CHECK();
     }
     return BBJD_SUCCESS;
 }
 
-template <int BS, int R>
+template <int BS, int R, typename T>
 static bbjd_status precond_apply(const bbjd_precond *pc, const cplx *r, cplx *x, int64_t stride,
                                  cudaStream_t st) {
     const int cap = 16 * num_sms();
     if (pc->kind == BBJD_PC_BLOCK_JACOBI) {
         const int64_t items = (pc->nblk + (32 / BS) - 1) / (32 / BS);
-        k_bjac<BS, R><<<grid_for(items, 8, cap), 256, 0, st>>>(pc->nblk, pc->pool, r, stride, x, stride);
+        k_bjac<BS, R, T><<<grid_for(items, 8, cap), 256, 0, st>>>(pc->nblk, fac<T>(pc, pc->pool_base), r,
+                                                                 stride, x, stride);
         BBJD_LAUNCH_CHECK();
         if (pc->t > 0) {
             k_corner<R><<<1, 256, 0, st>>>(pc->nb, pc->t, pc->Ginv, r, stride, x, stride);
@@ -638,27 +814,49 @@ static bbjd_status precond_apply(const bbjd_precond *pc, const cplx *r, cplx *x,
         }
         return BBJD_SUCCESS;
     }
-    bbjd_status s = bcr_solve<BS, R>(pc, r, stride, x, stride, st);
+    bbjd_status s = bcr_solve<BS, R, T>(pc, r, stride, x, stride, st);
     if (s != BBJD_SUCCESS || pc->t == 0) return s;
     const size_t smem = sizeof(cplx) * 8 * R * (size_t)pc->t;
-    k_border_g<R><<<pc->G, 256, smem, st>>>(pc->nb, pc->t, pc->FT, x, stride, pc->tau_part);
+    const int nq = (pc->t + 31) / 32;
+    const T *FT, *Y;
+    if constexpr (std::is_same<T, float2>::value) {
+        FT = pc->FT32;
+        Y = pc->Y32;
+    } else {
+        FT = pc->FT;
+        Y = pc->Y;
+    }
+    if (nq <= 1)
+        k_border_g<R, 1, T><<<pc->G, 256, smem, st>>>(pc->nb, pc->t, FT, x, stride, pc->tau_part);
+    else if (nq == 2)
+        k_border_g<R, 2, T><<<pc->G, 256, smem, st>>>(pc->nb, pc->t, FT, x, stride, pc->tau_part);
+    else
+        k_border_g<R, 4, T><<<pc->G, 256, smem, st>>>(pc->nb, pc->t, FT, x, stride, pc->tau_part);
     BBJD_LAUNCH_CHECK();
-    k_border_x2<R><<<1, 256, 0, st>>>(pc->nb, pc->t, pc->G, pc->tau_part, pc->Sinv, r, stride, x,
-                                      stride, pc->x2);
+    k_border_gsum<R><<<(unsigned)((R * pc->t + 7) / 8), 256, 0, st>>>(pc->nb, pc->t, pc->G,
+                                                                       pc->tau_part, r, stride, pc->gbuf);
     BBJD_LAUNCH_CHECK();
-    k_border_x1<R><<<grid_for(pc->nb, 256, 8 * num_sms()), 256, 0, st>>>(pc->nb, pc->t, pc->Y, pc->x2,
-                                                                        x, stride);
+    k_border_x2<R><<<(unsigned)((R * pc->t + 255) / 256), 256, 0, st>>>(pc->nb, pc->t, pc->gbuf,
+                                                                         pc->Sinv, x, stride, pc->x2);
+    BBJD_LAUNCH_CHECK();
+    k_border_x1<R, T><<<grid_for(pc->nb, 256, 8 * num_sms()), 256, 0, st>>>(pc->nb, pc->t, Y, pc->x2,
+                                                                           x, stride);
     BBJD_LAUNCH_CHECK();
     return BBJD_SUCCESS;
 }
 
 bbjd_status precond_solve(const bbjd_precond *pc, int nrhs, const cplx *r, cplx *x, int64_t stride,
                           cudaStream_t st) {
-#define BBJD_PC(BS)                                                   \
-    if (pc->b == BS) {                                                \
-        if (nrhs == 1) return precond_apply<BS, 1>(pc, r, x, stride, st); \
-        if (nrhs == 2) return precond_apply<BS, 2>(pc, r, x, stride, st); \
-        return BBJD_ERR_INVALID;                                      \
+    const bool c64 = pc->precision == BBJD_MIXED;
+#define BBJD_PC(BS)                                                                       \
+    if (pc->b == BS) {                                                                    \
+        if (nrhs == 1)                                                                    \
+            return c64 ? precond_apply<BS, 1, float2>(pc, r, x, stride, st)               \
+                       : precond_apply<BS, 1, cplx>(pc, r, x, stride, st);                \
+        if (nrhs == 2)                                                                    \
+            return c64 ? precond_apply<BS, 2, float2>(pc, r, x, stride, st)               \
+                       : precond_apply<BS, 2, cplx>(pc, r, x, stride, st);                \
+        return BBJD_ERR_INVALID;                                                          \
     }
     BBJD_PC(8)
     BBJD_PC(16)
@@ -668,7 +866,8 @@ bbjd_status precond_solve(const bbjd_precond *pc, int nrhs, const cplx *r, cplx 
 }
 
 double precond_bytes(const bbjd_precond *pc, int nrhs) {
-    const double bb = 16.0 * pc->b * pc->b;
+    const double es = pc->precision == BBJD_MIXED ? 8.0 : 16.0;  // bytes per stored factor entry
+    const double bb = es * pc->b * pc->b;
     double bytes = 0.0;
     if (pc->kind == BBJD_PC_BLOCK_JACOBI) {
         bytes = bb * pc->nblk + 16.0 * pc->t * pc->t;
@@ -682,7 +881,7 @@ double precond_bytes(const bbjd_precond *pc, int nrhs) {
     }
     bytes += bb;  // top
     if (pc->t > 0) {
-        bytes += 16.0 * (double)pc->nb * pc->t * 2.0;        // F1 and Y
+        bytes += es * (double)pc->nb * pc->t * 2.0;          // F1 and Y
         bytes += 16.0 * nrhs * (double)pc->nb * 3.0;         // y read twice, x1 written
     }
     return bytes;
@@ -721,6 +920,8 @@ static bbjd_status factor_bcr(bbjd_precond *pc, const bbjd_bbt_matrix *m, cplx s
     pc->top_off = off;
     pc->lvl_total = off + BS;
     BBJD_CUDA_TRY(cudaMalloc(&pc->pool, sizeof(cplx) * BB * pool_blocks));
+    pc->pool_elems = BB * pool_blocks;
+    pc->pool_base = pc->pool;
     BBJD_CUDA_TRY(cudaMalloc(&pc->lvl_rhs, sizeof(cplx) * 2 * pc->lvl_total));
     BBJD_CUDA_TRY(cudaMalloc(&pc->lvl_x, sizeof(cplx) * 2 * pc->lvl_total));
     cplx *p = pc->pool;
@@ -805,6 +1006,8 @@ static bbjd_status factor_bjac(bbjd_precond *pc, const bbjd_bbt_matrix *m, cplx 
     constexpr int64_t BB = BS * BS;
     BBJD_CUDA_TRY(cudaMemsetAsync(pc->err, 0, sizeof(int), st));
     BBJD_CUDA_TRY(cudaMalloc(&pc->pool, sizeof(cplx) * BB * pc->nblk));
+    pc->pool_elems = BB * pc->nblk;
+    pc->pool_base = pc->pool;
     cplx *D = nullptr;
     BBJD_CUDA_TRY(cudaMalloc(&D, sizeof(cplx) * BB * pc->nblk));
     k_shift<<<grid_for(BB * pc->nblk, 256, 8 * num_sms()), 256, 0, st>>>(BB * pc->nblk, m->Ad, m->Bd, sigma, D);
@@ -829,12 +1032,40 @@ static bbjd_status factor_bjac(bbjd_precond *pc, const bbjd_bbt_matrix *m, cplx 
 
 }  // namespace bbjd
 
+namespace bbjd {
+// Mixed precision: keep complex64 copies of the factor blocks, of Y = K^-1 E
+// and of the tau rows (the solve reads them, widening to FP64 for the
+// arithmetic), and release the FP64 factor blocks and Y.  The factorisation
+// itself ran in FP64.
+static bbjd_status to_complex64(bbjd_precond *pc, const bbjd_bbt_matrix *m) {
+    const int cap = 8 * num_sms();
+    BBJD_CUDA_TRY(cudaMalloc(&pc->pool32, sizeof(float2) * (size_t)pc->pool_elems));
+    k_to_c64<<<grid_for(pc->pool_elems, 256, cap), 256>>>(pc->pool_elems, pc->pool, pc->pool32);
+    BBJD_LAUNCH_CHECK();
+    if (pc->Y) {
+        const int64_t ny = pc->nb * pc->t, nf = m->n * m->t;
+        BBJD_CUDA_TRY(cudaMalloc(&pc->Y32, sizeof(float2) * (size_t)ny));
+        BBJD_CUDA_TRY(cudaMalloc(&pc->FT32, sizeof(float2) * (size_t)nf));
+        k_to_c64<<<grid_for(ny, 256, cap), 256>>>(ny, pc->Y, pc->Y32);
+        BBJD_LAUNCH_CHECK();
+        k_to_c64<<<grid_for(nf, 256, cap), 256>>>(nf, m->FT, pc->FT32);
+        BBJD_LAUNCH_CHECK();
+    }
+    BBJD_CUDA_TRY(cudaDeviceSynchronize());
+    cudaFree(pc->pool);
+    pc->pool = nullptr;   // pool_base keeps the offsets
+    cudaFree(pc->Y);
+    pc->Y = nullptr;
+    return BBJD_SUCCESS;
+}
+}  // namespace bbjd
+
 using namespace bbjd;
 
 extern "C" bbjd_status bbjd_precond_create(const bbjd_bbt_matrix *m, bbjd_zomplex sigma, int kind,
                                            int precision, bbjd_precond **out) {
     if (!m || !out || (kind != BBJD_PC_BBT_LU && kind != BBJD_PC_BLOCK_JACOBI)) return BBJD_ERR_INVALID;
-    if (precision != BBJD_FP64) return BBJD_ERR_INVALID;  // complex64 factors: not built yet
+    if (precision != BBJD_FP64 && precision != BBJD_MIXED) return BBJD_ERR_INVALID;
     auto t0 = std::chrono::steady_clock::now();
     auto *pc = new bbjd_precond();
     pc->kind = kind;
@@ -849,17 +1080,22 @@ extern "C" bbjd_status bbjd_precond_create(const bbjd_bbt_matrix *m, bbjd_zomple
     cudaStream_t st = nullptr;
     bbjd_status s = BBJD_SUCCESS;
     if (cudaMalloc(&pc->err, sizeof(int)) != cudaSuccess) s = BBJD_ERR_ALLOC;
+    static std::mutex attr_mu;
     static bool attrs = false;
-    if (s == BBJD_SUCCESS && !attrs) {
-        s = set_attrs<8>();
-        if (s == BBJD_SUCCESS) s = set_attrs<16>();
-        if (s == BBJD_SUCCESS) s = set_attrs<32>();
-        attrs = (s == BBJD_SUCCESS);
+    if (s == BBJD_SUCCESS) {
+        std::lock_guard<std::mutex> lock(attr_mu);
+        if (!attrs) {
+            s = set_attrs<8>();
+            if (s == BBJD_SUCCESS) s = set_attrs<16>();
+            if (s == BBJD_SUCCESS) s = set_attrs<32>();
+            attrs = (s == BBJD_SUCCESS);
+        }
     }
     if (s == BBJD_SUCCESS) {
         pc->G = (int)std::max<int64_t>(1, std::min<int64_t>(4 * num_sms(), (m->nb + 255) / 256));
         if (cudaMalloc(&pc->tau_part, sizeof(cplx) * (size_t)pc->G * 2 * std::max(1, m->t)) != cudaSuccess ||
-            cudaMalloc(&pc->x2, sizeof(cplx) * 2 * std::max(1, m->t)) != cudaSuccess)
+            cudaMalloc(&pc->x2, sizeof(cplx) * 2 * std::max(1, m->t)) != cudaSuccess ||
+            cudaMalloc(&pc->gbuf, sizeof(cplx) * 2 * std::max(1, m->t)) != cudaSuccess)
             s = BBJD_ERR_ALLOC;
     }
     if (s == BBJD_SUCCESS) {
@@ -874,6 +1110,7 @@ extern "C" bbjd_status bbjd_precond_create(const bbjd_bbt_matrix *m, bbjd_zomple
         }
     }
     if (s == BBJD_SUCCESS && cudaDeviceSynchronize() != cudaSuccess) s = BBJD_ERR_CUDA;
+    if (s == BBJD_SUCCESS && precision == BBJD_MIXED) s = to_complex64(pc, m);
     if (s != BBJD_SUCCESS) {
         bbjd_precond_free(pc);
         return s;
@@ -886,13 +1123,17 @@ extern "C" bbjd_status bbjd_precond_create(const bbjd_bbt_matrix *m, bbjd_zomple
 extern "C" void bbjd_precond_free(bbjd_precond *pc) {
     if (!pc) return;
     cudaFree(pc->pool);
+    cudaFree(pc->pool32);
     cudaFree(pc->Y);
+    cudaFree(pc->Y32);
+    cudaFree(pc->FT32);
     cudaFree(pc->Sinv);
     cudaFree(pc->Ginv);
     cudaFree(pc->lvl_rhs);
     cudaFree(pc->lvl_x);
     cudaFree(pc->tau_part);
     cudaFree(pc->x2);
+    cudaFree(pc->gbuf);
     cudaFree(pc->err);
     delete pc;
 }

@@ -121,81 +121,110 @@ __global__ void __launch_bounds__(256) k_bbt_spmv(
 }
 
 // Tau rows and the residual norm: y[nb + tau] = sum_g tau_part[g][tau] +
-// F[tau, nb:] x[nb:]; B's tau rows are zero.  1024 threads: `slices` threads
-// per tau sum disjoint CTA ranges, then combine in a fixed order.
-__global__ void __launch_bounds__(1024) k_bbt_tau_finalize(
+// F[tau, nb:] x[nb:], one warp per tau row (lanes over the CTA partials, a
+// fixed order); B's tau rows are zero.  With a residual, the last CTA to
+// finish adds the interior partial norms and the tau rows' |r|^2 in a fixed
+// order and stores ||r||.
+__global__ void __launch_bounds__(256) k_bbt_tau_finalize(
     int t, int64_t nb, int G, const cplx *__restrict__ tau_part, const cplx *__restrict__ FT,
     const cplx *__restrict__ x, cplx *__restrict__ yA, cplx *__restrict__ yB, cplx ta, cplx tb,
-    cplx *__restrict__ r, const double *__restrict__ rn_part, double *__restrict__ rnorm) {
-    __shared__ cplx part[1024];
-    __shared__ double rpart[1024];
-    const int tid = threadIdx.x;
-    double rs = 0.0;
-    for (int g = tid; g < G; g += blockDim.x) rs += rn_part[g];
-    rpart[tid] = rs;
-    if (t > 0) {
-        const int slices = max(1, (int)blockDim.x / t);
-        const int tau = tid % t, sl = tid / t;
+    cplx *__restrict__ r, const double *__restrict__ rn_part, double *__restrict__ rtau_nsq,
+    unsigned *counter, double *__restrict__ rnorm) {
+    const int lane = threadIdx.x & 31;
+    const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (w < t) {
         cplx s = mk(0.0, 0.0);
-        if (sl < slices) {
-            for (int g = sl; g < G; g += slices) s = cadd(s, tau_part[(int64_t)g * t + tau]);
-            if (sl == 0)
-                for (int c = 0; c < t; ++c) cfma(s, FT[(nb + c) * t + tau], x[nb + c]);
-        }
-        part[tid] = s;
-        __syncthreads();
-        if (tid < t) {
-            cplx tot = part[tid];
-            for (int k = 1; k < slices; ++k) tot = cadd(tot, part[k * t + tid]);
-            yA[nb + tid] = tot;
-            yB[nb + tid] = mk(0.0, 0.0);
+        for (int g = lane; g < G; g += 32) s = cadd(s, tau_part[(int64_t)g * t + w]);
+        for (int c = lane; c < t; c += 32) cfma(s, FT[(nb + c) * t + w], x[nb + c]);
+        s = warp_sum(s);
+        if (lane == 0) {
+            yA[nb + w] = s;
+            yB[nb + w] = mk(0.0, 0.0);
             if (r) {
-                const cplx rr = cmul(tb, tot);
-                r[nb + tid] = rr;
-                rpart[tid] += cabs2(rr);
+                const cplx rr = cmul(tb, s);
+                r[nb + w] = rr;
+                rtau_nsq[w] = cabs2(rr);
             }
         }
     }
+    if (!r) return;
+    __shared__ bool last;
+    __shared__ double red[8];
+    __threadfence();
     __syncthreads();
-    __shared__ double wsum[32];
-    const double w = warp_sum(rpart[tid]);
-    if ((tid & 31) == 0) wsum[tid >> 5] = w;
+    if (threadIdx.x == 0) last = (atomicAdd(counter, 1u) == gridDim.x - 1);
     __syncthreads();
-    if (tid == 0 && r) {
+    if (!last) return;
+    double acc = 0.0;
+    for (int g = threadIdx.x; g < G; g += blockDim.x) acc += __ldcg(rn_part + g);
+    for (int i = threadIdx.x; i < t; i += blockDim.x) acc += __ldcg(rtau_nsq + i);
+    acc = warp_sum(acc);
+    if (lane == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
         double tot = 0.0;
-        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) tot += wsum[i];
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) tot += red[i];
         *rnorm = sqrt(tot);
+        *counter = 0u;
     }
 }
 
 template <int BS>
-static bbjd_status launch_spmv(const bbjd_bbt_matrix *m, const cplx *x, cplx *yA, cplx *yB,
-                               cplx ta, cplx tb, cplx *r, double *rnorm, cudaStream_t st) {
+static bbjd_status launch_spmv(const bbjd_bbt_matrix *m, const BBTScratch *sc, const cplx *x,
+                               cplx *yA, cplx *yB, cplx ta, cplx tb, cplx *r, double *rnorm,
+                               cudaStream_t st) {
     const size_t smem = sizeof(cplx) * (size_t)m->t * 9;
     const int nq = (m->t + 31) / 32;
 #define BBJD_SPMV(NQ)                                                                   \
-    k_bbt_spmv<BS, NQ><<<m->G, 256, smem, st>>>(m->nblk, m->t, m->nb, m->Ad, m->Al, m->Au, \
+    k_bbt_spmv<BS, NQ><<<sc->G, 256, smem, st>>>(m->nblk, m->t, m->nb, m->Ad, m->Al, m->Au, \
                                                  m->Bd, m->E, m->FT, x, yA, yB, ta, tb, r,  \
-                                                 m->tau_part, m->rn_part)
+                                                 sc->tau_part, sc->rn_part)
     if (nq <= 1) BBJD_SPMV(1);
     else if (nq == 2) BBJD_SPMV(2);
     else if (nq <= 4) BBJD_SPMV(4);
     else return BBJD_ERR_INVALID;
 #undef BBJD_SPMV
     BBJD_LAUNCH_CHECK();
-    k_bbt_tau_finalize<<<1, 1024, 0, st>>>(m->t, m->nb, m->G, m->tau_part, m->FT, x, yA, yB, ta,
-                                           tb, r, m->rn_part, rnorm);
+    if (m->t > 0 || r) {
+        const unsigned gf = (unsigned)std::max(1, (m->t + 7) / 8);
+        k_bbt_tau_finalize<<<gf, 256, 0, st>>>(m->t, m->nb, sc->G, sc->tau_part, m->FT, x, yA, yB, ta,
+                                               tb, r, sc->rn_part, sc->rtau_nsq, sc->counter, rnorm);
+    }
     BBJD_LAUNCH_CHECK();
     return BBJD_SUCCESS;
 }
 
-bbjd_status bbt_apply(const bbjd_bbt_matrix *m, const cplx *x, cplx *yA, cplx *yB, cplx ta,
-                      cplx tb, cplx *r, double *rnorm, cudaStream_t st) {
-    if (!rnorm) rnorm = m->rnorm;
+bbjd_status bbt_scratch_alloc(const bbjd_bbt_matrix *m, BBTScratch *sc) {
+    const int BPW = 32 / m->b;
+    const int64_t groups = (m->nblk + BPW - 1) / BPW;
+    const int t = m->t;
+    sc->G = (int)std::max<int64_t>(1, std::min<int64_t>(4 * num_sms(), (groups + 7) / 8));
+    BBJD_CUDA_TRY(cudaMalloc(&sc->tau_part, sizeof(cplx) * (size_t)sc->G * (t > 0 ? t : 1)));
+    BBJD_CUDA_TRY(cudaMalloc(&sc->rn_part, sizeof(double) * (size_t)sc->G));
+    BBJD_CUDA_TRY(cudaMalloc(&sc->rnorm, sizeof(double)));
+    BBJD_CUDA_TRY(cudaMalloc(&sc->rtau_nsq, sizeof(double) * (size_t)(t > 0 ? t : 1)));
+    BBJD_CUDA_TRY(cudaMalloc(&sc->counter, sizeof(unsigned)));
+    BBJD_CUDA_TRY(cudaMemset(sc->counter, 0, sizeof(unsigned)));
+    return BBJD_SUCCESS;
+}
+
+void bbt_scratch_free(BBTScratch *sc) {
+    cudaFree(sc->tau_part);
+    cudaFree(sc->rn_part);
+    cudaFree(sc->rnorm);
+    cudaFree(sc->rtau_nsq);
+    cudaFree(sc->counter);
+    *sc = BBTScratch();
+}
+
+bbjd_status bbt_apply(const bbjd_bbt_matrix *m, const BBTScratch *sc, const cplx *x, cplx *yA,
+                      cplx *yB, cplx ta, cplx tb, cplx *r, double *rnorm, cudaStream_t st) {
+    if (!sc) sc = &m->sc;
+    if (!rnorm) rnorm = sc->rnorm;
     switch (m->b) {
-        case 8: return launch_spmv<8>(m, x, yA, yB, ta, tb, r, rnorm, st);
-        case 16: return launch_spmv<16>(m, x, yA, yB, ta, tb, r, rnorm, st);
-        case 32: return launch_spmv<32>(m, x, yA, yB, ta, tb, r, rnorm, st);
+        case 8: return launch_spmv<8>(m, sc, x, yA, yB, ta, tb, r, rnorm, st);
+        case 16: return launch_spmv<16>(m, sc, x, yA, yB, ta, tb, r, rnorm, st);
+        case 32: return launch_spmv<32>(m, sc, x, yA, yB, ta, tb, r, rnorm, st);
         default: return BBJD_ERR_INVALID;
     }
 }
@@ -254,12 +283,7 @@ extern "C" bbjd_status bbjd_bbt_create(bbjd_int b, bbjd_int nblk, bbjd_int t,
     // the couplings outside the matrix are zero by definition
     ok = ok && cudaMemset(m->Al, 0, blk) == cudaSuccess &&
          cudaMemset(m->Au + (size_t)(nblk - 1) * b * b, 0, blk) == cudaSuccess;
-    const int BPW = 32 / (int)b;
-    const int64_t groups = (nblk + BPW - 1) / BPW;
-    m->G = (int)std::max<int64_t>(1, std::min<int64_t>(4 * num_sms(), (groups + 7) / 8));
-    ok = ok && cudaMalloc(&m->tau_part, sizeof(cplx) * (size_t)m->G * (t > 0 ? t : 1)) == cudaSuccess &&
-         cudaMalloc(&m->rn_part, sizeof(double) * (size_t)m->G) == cudaSuccess &&
-         cudaMalloc(&m->rnorm, sizeof(double)) == cudaSuccess;
+    ok = ok && bbt_scratch_alloc(m, &m->sc) == BBJD_SUCCESS;
     if (!ok) {
         bbjd_bbt_free(m);
         return BBJD_ERR_CUDA;
@@ -271,9 +295,7 @@ extern "C" bbjd_status bbjd_bbt_create(bbjd_int b, bbjd_int nblk, bbjd_int t,
 extern "C" void bbjd_bbt_free(bbjd_bbt_matrix *m) {
     if (!m) return;
     cudaFree(m->mem);
-    cudaFree(m->tau_part);
-    cudaFree(m->rn_part);
-    cudaFree(m->rnorm);
+    bbt_scratch_free(&m->sc);
     delete m;
 }
 
@@ -286,7 +308,7 @@ extern "C" double bbjd_bbt_matvec_bytes(const bbjd_bbt_matrix *m) {
 extern "C" bbjd_status bbjd_bbt_matvec(const bbjd_bbt_matrix *m, const bbjd_zomplex *x,
                                        bbjd_zomplex *yA, bbjd_zomplex *yB, void *stream) {
     if (!m || !x || !yA || !yB) return BBJD_ERR_INVALID;
-    return bbt_apply(m, reinterpret_cast<const cplx *>(x), reinterpret_cast<cplx *>(yA),
+    return bbt_apply(m, nullptr, reinterpret_cast<const cplx *>(x), reinterpret_cast<cplx *>(yA),
                      reinterpret_cast<cplx *>(yB), mk(0, 0), mk(0, 0), nullptr, nullptr,
                      (cudaStream_t)stream);
 }

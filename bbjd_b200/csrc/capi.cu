@@ -6,6 +6,8 @@
 #include <cstdlib>
 #include <cstring>
 #include <new>
+#include <thread>
+#include <atomic>
 
 namespace bbjd {
 
@@ -15,10 +17,12 @@ struct DeviceOps : Operators {
     const bbjd_bbt_matrix *m;
     const bbjd_precond *pc;
     cudaStream_t st;
+    BBTScratch sc;   // this solve's own product scratch
     DeviceOps(const bbjd_bbt_matrix *m_, const bbjd_precond *pc_, cudaStream_t s) : m(m_), pc(pc_), st(s) {}
+    ~DeviceOps() override { bbt_scratch_free(&sc); }
     bbjd_status apply(const cplx *x, cplx *yA, cplx *yB, cplx ta, cplx tb, cplx *r,
                       double *rnorm_dev) override {
-        return bbt_apply(m, x, yA, yB, ta, tb, r, rnorm_dev, st);
+        return bbt_apply(m, &sc, x, yA, yB, ta, tb, r, rnorm_dev, st);
     }
     bool has_precond() const override { return pc != nullptr; }
     bbjd_status precond(int nrhs, const cplx *r, cplx *x) override {
@@ -30,7 +34,12 @@ struct DeviceOps : Operators {
 
 Operators *make_device_ops(const bbjd_bbt_matrix *m, const bbjd_precond *pc, Scratch *,
                            cudaStream_t st) {
-    return new (std::nothrow) DeviceOps(m, pc, st);
+    auto *o = new (std::nothrow) DeviceOps(m, pc, st);
+    if (o && bbt_scratch_alloc(m, &o->sc) != BBJD_SUCCESS) {
+        delete o;
+        return nullptr;
+    }
+    return o;
 }
 
 // Host callbacks (the reference's operator interface, include/bbjd.h:101-109):
@@ -289,7 +298,8 @@ bbjd_status bbjd_solve_device(const bbjd_params *params, bbjd_device_ext *ext,
     memset(result, 0, sizeof(*result));
     if (!params_ok(params, ws) || !m || m->n != params->n) return result->status = BBJD_ERR_INVALID;
     if (pc && pc->n != m->n) return result->status = BBJD_ERR_INVALID;
-    if (ext && ext->precision != BBJD_FP64) return result->status = BBJD_ERR_INVALID;
+    if (ext && ext->precision != BBJD_FP64 && ext->precision != BBJD_MIXED)
+        return result->status = BBJD_ERR_INVALID;
     bbjd_status s = alloc_result(params, result);
     if (s) return result->status = s;
     cudaStream_t st = ext ? (cudaStream_t)ext->stream : nullptr;
@@ -306,6 +316,44 @@ bbjd_status bbjd_solve_device(const bbjd_params *params, bbjd_device_ext *ext,
     delete ops;
     if (own) cudaStreamDestroy(st);
     return s;
+}
+
+bbjd_status bbjd_solve_batch(int count, const bbjd_params *params, bbjd_device_ext *exts,
+                             const bbjd_bbt_matrix *const *mats, const bbjd_precond *const *pcs,
+                             bbjd_workspace *const *wss, bbjd_result *results, int threads) {
+    if (count < 0 || (count > 0 && (!params || !mats || !pcs || !wss || !results)) || threads < 1)
+        return BBJD_ERR_INVALID;
+    for (int i = 0; i < count; ++i) {
+        if (!params[i].v0 || !mats[i] || !wss[i]) return BBJD_ERR_INVALID;
+        for (int j = 0; j < i; ++j)
+            if (mats[j] == mats[i] || (pcs[i] && pcs[j] == pcs[i]) || wss[j] == wss[i])
+                return BBJD_ERR_INVALID;
+    }
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return BBJD_ERR_CUDA;
+    std::atomic<int> next{0};
+    std::vector<bbjd_status> st(count, BBJD_SUCCESS);
+    auto worker = [&]() {
+        cudaSetDevice(dev);
+        for (;;) {
+            const int i = next.fetch_add(1);
+            if (i >= count) break;
+            bbjd_device_ext local;
+            bbjd_device_ext_init(&local);
+            bbjd_device_ext *e = exts ? &exts[i] : &local;
+            st[i] = bbjd_solve_device(&params[i], e, mats[i], pcs[i], wss[i], &results[i]);
+        }
+    };
+    const int nt = std::min(threads, std::max(count, 1));
+    std::vector<std::thread> pool;
+    for (int t = 0; t < nt; ++t) pool.emplace_back(worker);
+    for (auto &th : pool) th.join();
+    bbjd_status out = BBJD_SUCCESS;
+    for (int i = 0; i < count; ++i) {
+        if (st[i] < 0) return st[i];
+        if (st[i] == BBJD_MAX_ITER) out = BBJD_MAX_ITER;
+    }
+    return out;
 }
 
 // Reference jd_core.c:244-266 on host arrays (staged through the device).

@@ -15,18 +15,27 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <mutex>
 
 namespace bbjd {
+
+// Basis loads: FP64, or the complex64 shadow of the mixed-precision form
+// widened to FP64.
+__device__ __forceinline__ cplx ldq(const double2 *p) { return __ldcs(p); }
+__device__ __forceinline__ cplx ldq(const float2 *p) {
+    const float2 f = __ldcs(p);
+    return mk((double)f.x, (double)f.y);
+}
 
 // ---------------------------------------------------------------------------
 // Stage 1 of Q^H v: partial[g][x] for x = (m*NV + p)*ncols + j, plus the
 // squared norms of the vectors at x = NM*NV*ncols + p.
 // One CTA owns a contiguous row range; its slice of each vector is staged in
 // shared memory once; warp w streams columns j = w, w + nwarps, ... of Q.
-template <int NM, int NV>
+template <int NM, int NV, typename QT = cplx>
 __global__ void __launch_bounds__(256) k_tsdot(int64_t n, int ncols, int64_t ld,
-                                               const cplx *__restrict__ Q0,
-                                               const cplx *__restrict__ Q1,
+                                               const QT *__restrict__ Q0,
+                                               const QT *__restrict__ Q1,
                                                const cplx *__restrict__ v0,
                                                const cplx *__restrict__ v1, int64_t rpc,
                                                cplx *__restrict__ partial, const int *flag) {
@@ -67,14 +76,14 @@ __global__ void __launch_bounds__(256) k_tsdot(int64_t n, int ncols, int64_t ld,
 
     for (int cj = warp; cj < NM * ncols; cj += nwarps) {
         const int m = cj / ncols, j = cj - m * ncols;
-        const cplx *q = ((NM > 1 && m == 1) ? Q1 : Q0) + (int64_t)j * ld + r0;
+        const QT *q = ((NM > 1 && m == 1) ? Q1 : Q0) + (int64_t)j * ld + r0;
         cplx acc[NV];
 #pragma unroll
         for (int p = 0; p < NV; ++p) acc[p] = mk(0.0, 0.0);
         int i = lane;
         for (; i + 96 < nr; i += 128) {
-            cplx q0 = ldg_stream(q + i), q1 = ldg_stream(q + i + 32);
-            cplx q2 = ldg_stream(q + i + 64), q3 = ldg_stream(q + i + 96);
+            cplx q0 = ldq(q + i), q1 = ldq(q + i + 32);
+            cplx q2 = ldq(q + i + 64), q3 = ldq(q + i + 96);
 #pragma unroll
             for (int p = 0; p < NV; ++p) {
                 const cplx *s = sv + p * rpc;
@@ -85,7 +94,7 @@ __global__ void __launch_bounds__(256) k_tsdot(int64_t n, int ncols, int64_t ld,
             }
         }
         for (; i < nr; i += 32) {
-            cplx qv = ldg_stream(q + i);
+            cplx qv = ldq(q + i);
 #pragma unroll
             for (int p = 0; p < NV; ++p) cfmac(acc[p], qv, sv[p * rpc + i]);
         }
@@ -105,8 +114,19 @@ __global__ void __launch_bounds__(256) k_reduce(const cplx *__restrict__ partial
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     const int x = blockIdx.x * 32 + tx;
     cplx acc = mk(0.0, 0.0);
-    if (x < X)
-        for (int g = ty; g < G; g += 8) acc = cadd(acc, partial[(int64_t)g * X + x]);
+    if (x < X) {
+        // four independent chains keep four loads in flight per thread
+        cplx a1 = mk(0.0, 0.0), a2 = mk(0.0, 0.0), a3 = mk(0.0, 0.0);
+        int g = ty;
+        for (; g + 24 < G; g += 32) {
+            acc = cadd(acc, partial[(int64_t)g * X + x]);
+            a1 = cadd(a1, partial[(int64_t)(g + 8) * X + x]);
+            a2 = cadd(a2, partial[(int64_t)(g + 16) * X + x]);
+            a3 = cadd(a3, partial[(int64_t)(g + 24) * X + x]);
+        }
+        for (; g < G; g += 8) acc = cadd(acc, partial[(int64_t)g * X + x]);
+        acc = cadd(cadd(acc, a1), cadd(a2, a3));
+    }
     s[ty][tx] = acc;
     __syncthreads();
     if (ty == 0 && x < X) {
@@ -123,8 +143,9 @@ __global__ void __launch_bounds__(256) k_reduce(const cplx *__restrict__ partial
 //   flag_out = ||v_out|| < 0.7071 ||v_before||       (reference jd_core.c:232)
 // where ||v_before||^2 is read from ref_nsq (the x = NM*NV*ncols slot the
 // first-pass dot kernel wrote).
+template <typename QT>
 __global__ void __launch_bounds__(256) k_update(
-    int64_t n, int ncols, int64_t ld, const cplx *__restrict__ Q, const cplx *__restrict__ h1,
+    int64_t n, int ncols, int64_t ld, const QT *__restrict__ Q, const cplx *__restrict__ h1,
     const cplx *__restrict__ h2, cplx c1, cplx c2, cplx a, const cplx *v_in, cplx b,
     const cplx *__restrict__ w_in, cplx *v_out, double *__restrict__ nrm_part,
     unsigned *counter, double *norm_out, const cplx *ref_nsq, const double *ref_nrm, int *flag_out,
@@ -143,16 +164,16 @@ __global__ void __launch_bounds__(256) k_update(
         cplx acc = mk(0.0, 0.0);
         if (v_in) acc = cmul(a, v_in[i]);
         if (w_in) cfma(acc, b, w_in[i]);
-        const cplx *q = Q + i;
+        const QT *q = Q + i;
         int j = 0;
         for (; j + 8 <= ncols; j += 8) {
             cplx qv[8];
 #pragma unroll
-            for (int u = 0; u < 8; ++u) qv[u] = ldg_stream(q + (int64_t)(j + u) * ld);
+            for (int u = 0; u < 8; ++u) qv[u] = ldq(q + (int64_t)(j + u) * ld);
 #pragma unroll
             for (int u = 0; u < 8; ++u) cfms(acc, qv[u], hs[j + u]);
         }
-        for (; j < ncols; ++j) cfms(acc, ldg_stream(q + (int64_t)j * ld), hs[j]);
+        for (; j < ncols; ++j) cfms(acc, ldq(q + (int64_t)j * ld), hs[j]);
         v_out[i] = acc;
         nsq += cabs2(acc);
     }
@@ -356,13 +377,14 @@ __global__ void __launch_bounds__(256) k_gram(int64_t n, int keep, const cplx *_
 std::atomic<long long> g_launches{0};
 
 int num_sms() {
+    static std::once_flag once;
     static int sms = 0;
-    if (!sms) {
-        int dev = 0;
+    std::call_once(once, [] {
+        int dev = 0, v = 0;
         cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (sms <= 0) sms = 148;
-    }
+        cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+        sms = v > 0 ? v : 148;
+    });
     return sms;
 }
 
@@ -496,6 +518,47 @@ bbjd_status gram(Scratch &S, int keep, const cplx *X, const cplx *Y, int64_t ldx
     BBJD_LAUNCH_CHECK();
     const int XX = keep * keep;
     k_reduce<<<(XX + 31) / 32, 256, 0, st>>>(partial, Gg, XX, out, nullptr);
+    BBJD_LAUNCH_CHECK();
+    return BBJD_SUCCESS;
+}
+
+// ---------------------------------------------------------------------------
+// Mixed-precision helpers: complex64 copies and passes over a complex64 basis.
+__global__ void k_cvt_c64(int64_t count, const double2 *__restrict__ in, float2 *__restrict__ out) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += stride)
+        out[i] = make_float2((float)in[i].x, (float)in[i].y);
+}
+
+bbjd_status to_c64(int64_t count, const cplx *in, float2 *out, cudaStream_t st) {
+    const int64_t g = std::min<int64_t>(8 * num_sms(), std::max<int64_t>(1, (count + 255) / 256));
+    k_cvt_c64<<<(unsigned)g, 256, 0, st>>>(count, in, out);
+    BBJD_LAUNCH_CHECK();
+    return BBJD_SUCCESS;
+}
+
+bbjd_status tsdot32(Scratch &S, int ncols, int64_t ld, const float2 *Q, const cplx *v, cplx *out,
+                    cudaStream_t st) {
+    const int X = ncols + 1;
+    if (X > S.maxX) return BBJD_ERR_INVALID;
+    static bool attr = false;
+    const size_t smem = sizeof(cplx) * (size_t)S.rpc;
+    if (!attr && smem > 48 * 1024) {
+        BBJD_CUDA_TRY(cudaFuncSetAttribute(k_tsdot<1, 1, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           227 * 1024));
+        attr = true;
+    }
+    k_tsdot<1, 1, float2><<<S.G, 256, smem, st>>>(S.n, ncols, ld, Q, Q, v, nullptr, S.rpc, S.partial, nullptr);
+    BBJD_LAUNCH_CHECK();
+    return reduce_partials(S.partial, S.G, X, out, st);
+}
+
+bbjd_status update32(Scratch &S, int ncols, int64_t ld, const float2 *Q, const cplx *h, cplx *v,
+                     double *norm_out, cudaStream_t st) {
+    const size_t smem = sizeof(cplx) * (size_t)std::max(ncols, 1);
+    k_update<float2><<<S.G2, 256, smem, st>>>(S.n, ncols, ld, Q, h, nullptr, mk(1, 0), mk(0, 0), mk(1, 0),
+                                              v, mk(0, 0), nullptr, v, S.nrm_part, S.counter, norm_out,
+                                              nullptr, nullptr, nullptr, nullptr);
     BBJD_LAUNCH_CHECK();
     return BBJD_SUCCESS;
 }

@@ -79,6 +79,8 @@ struct Engine {
     cplx *gram_out = nullptr;  // 2 x maxsub^2
     double *dscal = nullptr;   // device scalars
     int *dflag = nullptr;      // device flags
+    bool mixed = false;        // BBJD_MIXED: complex64 shadow of V for the first CGS pass
+    float2 *Vs = nullptr;      // n x maxsub complex64 copy of V (ld n)
     cplx *pin = nullptr;       // pinned host staging for small results
     double *pin_d = nullptr;
     int *pin_i = nullptr;
@@ -115,6 +117,7 @@ struct Engine {
     // building blocks
     bbjd_status orthogonalize(const cplx *Q, int64_t ldq, int k, cplx *v, double *norm_dev,
                               int cls);
+    bbjd_status orthogonalize_mixed(int k, cplx *v, double *norm_dev);
     bbjd_status project_out(const cplx *Q, int k, cplx *v, int cls);
     bbjd_status deflation_append(int j, const cplx *u, const cplx *Au_, const cplx *Bu_);
     bbjd_status gmres(int ndefl, zc ta, zc tb, const cplx *r, cplx *z);

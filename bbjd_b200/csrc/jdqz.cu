@@ -136,6 +136,8 @@ bbjd_status Engine::init(const bbjd_params *p, bbjd_workspace *w, bbjd_result *r
     BBJD_CUDA_TRY(cudaMalloc(&dscal, sizeof(double) * SC_N));
     BBJD_CUDA_TRY(cudaMalloc(&dflag, sizeof(int) * FL_N));
     BBJD_CUDA_TRY(cudaMemset(dflag, 0, sizeof(int) * FL_N));
+    mixed = e && e->precision == BBJD_MIXED;
+    if (mixed) BBJD_CUDA_TRY(cudaMalloc(&Vs, sizeof(float2) * (size_t)n * maxsub));
     const size_t pin_c = 8 * (size_t)(maxsub + nev + 8);
     BBJD_CUDA_TRY(cudaMallocHost(&pin, sizeof(cplx) * pin_c));
     BBJD_CUDA_TRY(cudaMallocHost(&pin_d, sizeof(double) * 16));
@@ -160,6 +162,8 @@ void Engine::release() {
     cudaFree(g1); cudaFree(g2); cudaFree(g3);
     cudaFree(Zdev); cudaFree(xdev); cudaFree(gram_part); cudaFree(gram_out);
     cudaFree(dscal); cudaFree(dflag);
+    cudaFree(Vs);
+    Vs = nullptr;
     cudaFreeHost(pin); cudaFreeHost(pin_d); cudaFreeHost(pin_i);
     if (own_stream && st) cudaStreamDestroy(st);
     st = nullptr;
@@ -209,6 +213,34 @@ bbjd_status Engine::orthogonalize(const cplx *Q, int64_t ldq, int k, cplx *v, do
     T.end();
     bytes_dev += pass_bytes;
     return s;
+}
+
+// Mixed-precision CGS of v against V[:, 0:k]: pass 1 over the complex64
+// shadow Vs (half the bytes; leaves O(1e-7) components along V), pass 2 in
+// FP64 always, and the DGKS re-pass (FP64) when pass 2 still cancels more than
+// 0.7071 of the norm.  Same flag and norm slots as orthogonalize().
+bbjd_status Engine::orthogonalize_mixed(int k, cplx *v, double *norm_dev) {
+    if (k == 0) return orthogonalize(reinterpret_cast<cplx *>(ws->V), n, 0, v, norm_dev, KC_ORTH);
+    bbjd_status s;
+    const double b1 = 8.0 * n * (2.0 * k) + 16.0 * n * 3.0;
+    T.begin(KC_ORTH, b1 + 16.0 * (double)n * (2.0 * k + 3.0));
+    if ((s = tsdot32(S, k, n, Vs, v, S.red, st))) return s;
+    if ((s = update32(S, k, n, Vs, S.red, v, dscal + SC_TMP2, st))) return s;
+    const cplx *V = reinterpret_cast<const cplx *>(ws->V);
+    int *flag = dflag + FL_T;
+    cplx *h = S.red;
+    if ((s = tsdot(S, 1, 1, k, n, V, nullptr, v, nullptr, h, nullptr, st))) return s;
+    if ((s = update(S, k, n, V, h, nullptr, mk(1, 0), mk(0, 0), mk(1, 0), v, mk(0, 0), nullptr, v,
+                    norm_dev, nullptr, dscal + SC_TMP2, flag, nullptr, st)))
+        return s;
+    cplx *h2 = S.red + S.maxX;
+    if ((s = tsdot(S, 1, 1, k, n, V, nullptr, v, nullptr, h2, flag, st))) return s;
+    if ((s = update(S, k, n, V, h2, nullptr, mk(1, 0), mk(0, 0), mk(1, 0), v, mk(0, 0), nullptr, v,
+                    norm_dev, nullptr, nullptr, nullptr, flag, st)))
+        return s;
+    T.end();
+    bytes_dev += b1 + 16.0 * (double)n * (2.0 * k + 3.0);
+    return BBJD_SUCCESS;
 }
 
 // Two unconditional CGS passes (reference jd_core.c:269-309).
@@ -626,6 +658,7 @@ bbjd_status Engine::run() {
     }
     if (pin_d[0] < 1e-300) return res->status = BBJD_ERR_BREAKDOWN;
     if ((s = scale_by_norm(S, V, dscal + SC_VNORM, 0.0, V, st))) return s;
+    if (mixed && (s = to_c64(n, V, Vs, st))) return s;
     T.begin(KC_SPMV, abytes);
     s = ops->apply(V, AV, BV, mk(0, 0), mk(0, 0), nullptr, nullptr);  // jd_core.c:807-810
     T.end();
@@ -777,6 +810,7 @@ bbjd_status Engine::run() {
             const double gb = 16.0 * n * (double)(k + keep);
             T.begin(KC_RESTART, 3 * gb);
             if ((s = restart_gemm(n, (int)k, (int)keep, V, ld, Zdev, (int)k, V, st))) return s;
+            if (mixed && (s = to_c64(n * keep, V, Vs, st))) return s;
             if ((s = restart_gemm(n, (int)k, (int)keep, AV, ld, Zdev, (int)k, AV, st))) return s;
             if ((s = restart_gemm(n, (int)k, (int)keep, BV, ld, Zdev, (int)k, BV, st))) return s;
             T.end();
@@ -817,7 +851,9 @@ bbjd_status Engine::run() {
         } else {
             BBJD_CUDA_TRY(cudaMemcpyAsync(vnew, g3, sizeof(cplx) * n, cudaMemcpyDeviceToDevice, st));
         }
-        if ((s = orthogonalize(V, ld, (int)k, vnew, dscal + SC_VNORM, KC_ORTH))) return s;
+        if ((s = mixed ? orthogonalize_mixed((int)k, vnew, dscal + SC_VNORM)
+                       : orthogonalize(V, ld, (int)k, vnew, dscal + SC_VNORM, KC_ORTH)))
+            return s;
         BBJD_CUDA_TRY(cudaMemcpyAsync(pin_d + SC_VNORM, dscal + SC_VNORM, sizeof(double), cudaMemcpyDeviceToHost, st));
         BBJD_CUDA_TRY(cudaMemcpyAsync(pin_i + FL_T, dflag + FL_T, sizeof(int), cudaMemcpyDeviceToHost, st));
         if ((s = sync())) return s;
@@ -830,7 +866,9 @@ bbjd_status Engine::run() {
                 rv[i] = zc(re, im);
             }
             BBJD_CUDA_TRY(cudaMemcpyAsync(vnew, rv.data(), sizeof(cplx) * n, cudaMemcpyHostToDevice, st));
-            if ((s = orthogonalize(V, ld, (int)k, vnew, dscal + SC_VNORM, KC_ORTH))) return s;
+            if ((s = mixed ? orthogonalize_mixed((int)k, vnew, dscal + SC_VNORM)
+                       : orthogonalize(V, ld, (int)k, vnew, dscal + SC_VNORM, KC_ORTH)))
+            return s;
             BBJD_CUDA_TRY(cudaMemcpyAsync(pin_d + SC_VNORM, dscal + SC_VNORM, sizeof(double), cudaMemcpyDeviceToHost, st));
             if ((s = sync())) return s;
             if (pin_d[SC_VNORM] < 1e-14) {
@@ -840,6 +878,7 @@ bbjd_status Engine::run() {
             }
         }
         if ((s = scale_by_norm(S, vnew, dscal + SC_VNORM, 0.0, vnew, st))) return s;
+        if (mixed && (s = to_c64(n, vnew, Vs + k * ld, st))) return s;
         cplx *AVk = AV + k * ld, *BVk = BV + k * ld, *wnew = W + k * ld;
         T.begin(KC_SPMV, abytes);
         s = ops->apply(vnew, AVk, BVk, mk(0, 0), mk(0, 0), nullptr, nullptr);  // jd_core.c:1051-1054

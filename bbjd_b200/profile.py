@@ -27,14 +27,16 @@ def main(argv=None):
     ap.add_argument("--maxsub", type=int, default=200)
     ap.add_argument("--minsub", type=int, default=80)
     ap.add_argument("--projected", default="auto")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     a = ap.parse_args(argv)
     P = make_pencil(a.b, a.nblk, a.t, seed=0)
     dev = DevicePencil(P)
-    pc = DevicePreconditioner(dev, 3.0, "exact")
+    pc = DevicePreconditioner(dev, 3.0, "exact", precision=a.precision)
     t0 = time.time()
     ev, _, info = jdqz(dev, k=a.k, sigma=3.0, tol=1e-10, maxiter=a.iters, maxsub=a.maxsub,
                        minsub=a.minsub, preconditioner=pc, v0=start_vector(P.n, 1),
-                       return_info=True, timing=True, projected=a.projected)
+                       return_info=True, timing=True, projected=a.projected,
+                       precision=a.precision)
     wall = time.time() - t0
     d = info["device"]
     print(f"n={P.n} iters={info['iters']} nconv={info['nconv']} wall={wall:.2f}s "

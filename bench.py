@@ -44,10 +44,10 @@ WORKLOAD_NAME = "bbt_n1000064_k64"
 # Outer iterations per converged eigenpair of the FP64 device engine on this
 # pencil (same algorithm and start vector as the reference), used to turn
 # the reference's measured seconds per outer iteration into eigenpairs/s.
-PAIRS_PER_ITER = None
+PAIRS_PER_ITER = 12 / 2000   # measured: 12 pairs in the 2000-iteration cap (FP64, B200)
 # DRAM traffic (read + write bytes) per launch of the fused A,B product from
 # an ncu capture (profiles/), or None.
-SPMV_TRAFFIC_BYTES = None
+SPMV_TRAFFIC_BYTES = 4.149e9   # profiles/kernels_bbt_n131136.md, scaled by n
 
 
 def _env_rank():
@@ -224,10 +224,10 @@ def run_ours(args):
     gen_s = time.time() - t0
     solve_kw = dict(k=w["k"], sigma=w["sigma"], tol=w["tol"], maxiter=w["maxiter"],
                     maxsub=w["maxsub"], minsub=w["minsub"], v0=v0, return_info=True,
-                    projected=args.projected)
+                    projected=args.projected, precision=args.precision)
     dims = dict(b=w["b"], nblk=w["nblk"], t=w["t"])
     dev = DevicePencil(arrays=pinned, **dims)
-    pc = DevicePreconditioner(dev, w["sigma"], "exact")
+    pc = DevicePreconditioner(dev, w["sigma"], "exact", precision=args.precision)
     factor_s = pc.factor_seconds
 
     def barrier():
@@ -261,7 +261,7 @@ def run_ours(args):
     for _ in range(args.steps):
         def full():
             d = DevicePencil(arrays=pinned, **dims)
-            p = DevicePreconditioner(d, w["sigma"], "exact")
+            p = DevicePreconditioner(d, w["sigma"], "exact", precision=args.precision)
             r = jdqz(d, preconditioner=p, timing=False, **solve_kw)
             p.close()
             d.close()
@@ -305,8 +305,9 @@ def run_ours(args):
         "metric": "eigenpairs/s", "value": pairs_all / secs_max, "unit": "eigenpairs/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * secs_max / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "complex128", "data": "synthetic",
-        "config": {"workload": WORKLOAD_NAME, **WORKLOAD, "precision": "fp64",
+        "vs_baseline": None, "dtype": "complex128" if args.precision == "fp64" else "complex128+complex64",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD_NAME, **WORKLOAD, "precision": args.precision,
                    "projected": args.projected, "preconditioner": "exact block-bordered LU (device)",
                    "l2": "inputs larger than L2 (4.1 GB pencil), no flush"},
         "e2e": {"value": e_pairs_all / e_secs_max, "unit": "eigenpairs/s",
@@ -347,6 +348,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--projected", default="auto", choices=["auto", "qz", "schur"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
+                    help="fp64: the plain FP64 form; mixed: complex64 LU factors and first CGS pass")
     ap.add_argument("--ref-iters", type=int, default=6,
                     help="reference outer iterations per CPU sample step")
     ap.add_argument("--no-cpu-baseline", action="store_true")

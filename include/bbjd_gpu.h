@@ -124,6 +124,20 @@ bbjd_status bbjd_solve_device(const bbjd_params *params, bbjd_device_ext *ext,
                               const bbjd_bbt_matrix *m, const bbjd_precond *pc,
                               bbjd_workspace *ws, bbjd_result *result);
 
+/* Independent device solves of a sigma-sweep on one GPU (the reference's
+ * deployment runs one sigma per MPI rank, reference README.md:59-83): solve i
+ * uses params[i], mats[i], pcs[i] (may be NULL), wss[i], results[i] and, when
+ * exts != NULL, exts[i].  Up to `threads` solves run at once, each on its own
+ * host thread and CUDA stream, so the host-side projected QZ of one solve
+ * overlaps the device work of the others.  Every params[i].v0 must be set
+ * (the seeded start vector uses the C library's global rand()), and no two
+ * solves may share a matrix or preconditioner handle (their scratch is not
+ * shared-safe).  Returns the first failing status, else BBJD_SUCCESS (or
+ * BBJD_MAX_ITER if any solve stopped at maxiter). */
+bbjd_status bbjd_solve_batch(int count, const bbjd_params *params, bbjd_device_ext *exts,
+                             const bbjd_bbt_matrix *const *mats, const bbjd_precond *const *pcs,
+                             bbjd_workspace *const *wss, bbjd_result *results, int threads);
+
 /* ---- device kernels exposed for parity tests (device pointers) ---------- */
 
 /* CGS + DGKS of v (length n) against the k columns of Q (ld = ldq); returns

@@ -166,3 +166,28 @@ def test_gram_matches_numpy(n, keep):
     assert lib.bbjd_dev_gram(n, keep, Xd.data_ptr(), Yd.data_ptr(), n, Cm.ctypes.data, keep, None) == 0
     ref = X.conj().T @ Y
     assert np.abs(Cm - ref).max() < 1e-12 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("b,nblk,t", [(16, 256, 8), (32, 100, 64), (8, 33, 4)])
+@pytest.mark.parametrize("kind", ["exact", "block_jacobi"])
+def test_mixed_precision_preconditioner(b, nblk, t, kind):
+    """complex64 factors, FP64 vectors and arithmetic: the solve agrees with
+    the FP64 factors to complex64 accuracy (1e-5 relative here; the outer JD
+    iteration supplies the rest)."""
+    import torch
+    P = make_pencil(b, nblk, t, seed=8)
+    dev = DevicePencil(P)
+    sigma = 3.0 + 0.1j
+    p64 = DevicePreconditioner(dev, sigma, kind, precision="fp64")
+    p32 = DevicePreconditioner(dev, sigma, kind, precision="mixed")
+    assert p32.solve_bytes(2) < 0.85 * p64.solve_bytes(2)
+    r = np.stack([_rand(P.n, 1), _rand(P.n, 2)])
+    rd = _dev(r)
+    x64, x32 = torch.empty_like(rd), torch.empty_like(rd)
+    lib = _lib.load()
+    assert lib.bbjd_precond_solve(p64.handle, 2, rd.data_ptr(), x64.data_ptr(), None) == 0
+    assert lib.bbjd_precond_solve(p32.handle, 2, rd.data_ptr(), x32.data_ptr(), None) == 0
+    torch.cuda.synchronize()
+    a, c = _host(x64), _host(x32)
+    for q in range(2):
+        assert np.linalg.norm(c[q] - a[q]) / np.linalg.norm(a[q]) < 1e-5
