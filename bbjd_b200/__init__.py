@@ -5,8 +5,8 @@
 is loaded on first use; without it every solver call raises (there is no CPU
 compute path).
 """
-from .bbjd import DevicePencil, DevicePreconditioner, jdqz, jdqz_c  # noqa: F401
+from .bbjd import DevicePencil, DevicePreconditioner, jdqz, jdqz_batch, jdqz_c  # noqa: F401
 from .pencils import BBTPencil, make_pencil, start_vector  # noqa: F401
 
-__all__ = ["jdqz", "jdqz_c", "DevicePencil", "DevicePreconditioner", "BBTPencil",
+__all__ = ["jdqz", "jdqz_batch", "jdqz_c", "DevicePencil", "DevicePreconditioner", "BBTPencil",
            "make_pencil", "start_vector"]

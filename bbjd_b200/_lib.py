@@ -105,6 +105,9 @@ SIGNATURES = {
     "bbjd_device_ext_init": (None, [C.POINTER(DeviceExt)]),
     "bbjd_solve_device": (C.c_int, [C.POINTER(Params), C.POINTER(DeviceExt), C.c_void_p,
                                     C.c_void_p, C.POINTER(Workspace), C.POINTER(Result)]),
+    "bbjd_solve_batch": (C.c_int, [C.c_int, C.POINTER(Params), C.POINTER(DeviceExt),
+                                   C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
+                                   C.POINTER(C.POINTER(Workspace)), C.POINTER(Result), C.c_int]),
     "bbjd_dev_orthogonalize": (C.c_int, [bbjd_int, bbjd_int, C.c_void_p, bbjd_int, C.c_void_p,
                                          C.POINTER(C.c_double), C.POINTER(C.c_int), C.c_void_p]),
     "bbjd_dev_orthogonalize_static": (C.c_int, [bbjd_int, bbjd_int, C.c_void_p, bbjd_int,

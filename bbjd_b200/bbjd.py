@@ -426,3 +426,76 @@ def jdqz(
         return evals, evecs, {'nconv': nconv, 'iters': iters, 'status': status,
                               'residuals': resid}
     return evals, evecs
+
+
+def jdqz_batch(pencils, sigmas, k: int = 6, tol: float = 1e-10, maxiter: int = 200,
+               maxsub: int = 0, minsub: int = 0, preconditioner: str = "exact",
+               precision: str = "fp64", v0s=None, threads: int = 8, projected: str = "auto",
+               lock: str = "robust"):
+    """Independent 'nearest sigma' solves of a sigma-sweep on one GPU
+    (bbjd_solve_batch): solve i is ``jdqz(pencils[i], k=k, sigma=sigmas[i],
+    ...)``; up to `threads` run at once, each on its own host thread and
+    CUDA stream.  Returns a list of ``(eigenvalues, eigenvectors, info)``
+    and the batch's wall time in seconds.  Results equal those of the same
+    solves run one at a time."""
+    import time as _time
+    lib = _lib.load()
+    count = len(pencils)
+    if len(sigmas) != count:
+        raise ValueError("one sigma per pencil")
+    devs = [p if isinstance(p, DevicePencil) else DevicePencil(p) for p in pencils]
+    pcs = [DevicePreconditioner(d, s, preconditioner, precision=precision) if preconditioner
+           else None for d, s in zip(devs, sigmas)]
+    if v0s is None:
+        from .pencils import start_vector
+        v0s = [start_vector(d.n, 1 + i) for i, d in enumerate(devs)]
+    v0s = [np.ascontiguousarray(v, dtype=np.complex128) for v in v0s]
+    params = (_lib.Params * count)()
+    exts = (_lib.DeviceExt * count)()
+    mats = (C.c_void_p * count)(*[d.handle.value for d in devs])
+    pch = (C.c_void_p * count)(*[p.handle.value if p is not None else None for p in pcs])
+    wss = (C.POINTER(_lib.Workspace) * count)()
+    results = (_lib.Result * count)()
+    for i, (d, s) in enumerate(zip(devs, sigmas)):
+        p = params[i]
+        lib.bbjd_params_init(C.byref(p))
+        p.n, p.nev = d.n, int(k)
+        p.sigma = _lib.zcomplex.of(s)
+        p.tol, p.maxiter, p.maxsub, p.minsub = float(tol), int(maxiter), int(maxsub), int(minsub)
+        if v0s[i].shape != (d.n,):
+            raise ValueError(f"v0s[{i}] must have shape ({d.n},)")
+        p.v0 = v0s[i].ctypes.data
+        lib.bbjd_device_ext_init(C.byref(exts[i]))
+        exts[i].precision = 1 if precision == "mixed" else 0
+        exts[i].projected = _PROJECTED[projected]
+        exts[i].lock_rule = _LOCK[lock]
+        wss[i] = lib.bbjd_workspace_alloc(C.byref(p))
+        if not wss[i]:
+            for j in range(i):
+                lib.bbjd_workspace_free(wss[j])
+            raise MemoryError("bbjd_workspace_alloc failed (device memory)")
+    t0 = _time.perf_counter()
+    try:
+        status = lib.bbjd_solve_batch(count, params, exts, mats, pch, wss, results, int(threads))
+    finally:
+        wall = _time.perf_counter() - t0
+        for i in range(count):
+            lib.bbjd_workspace_free(wss[i])
+    if status < 0:
+        for i in range(count):
+            lib.bbjd_result_free(C.byref(results[i]))
+        raise RuntimeError(f"JDQZ batch failed: {_lib.STATUS_MSG.get(status, status)}")
+    out = []
+    for i, d in enumerate(devs):
+        try:
+            ev, evecs, resid = _marshal(results[i], d.n)
+        finally:
+            lib.bbjd_result_free(C.byref(results[i]))
+        out.append((ev, evecs, {"nconv": int(results[i].nconv), "iters": int(results[i].iters),
+                                "status": int(results[i].status), "residuals": resid,
+                                "seconds": exts[i].seconds_total,
+                                "seconds_qz": exts[i].seconds_qz}))
+    for p in pcs:
+        if p is not None:
+            p.close()
+    return out, wall

@@ -17,8 +17,34 @@ import time
 from . import DevicePencil, DevicePreconditioner, jdqz, make_pencil, start_vector
 
 
+def sweep(count: int, threads: int, precision: str, maxiter: int, seed: int = 7):
+    """The batched sweep: `count` pencils with b = t = 16 and n drawn
+    uniformly in [5e4, 3e5], sigma_j = 3 + i U[-40, 40], k = 16, maxsub 80,
+    minsub 32, solved concurrently on one GPU."""
+    import numpy as np
+
+    from . import jdqz_batch
+    rng = np.random.default_rng(seed)
+    ns = rng.uniform(5e4, 3e5, size=count)
+    sig = rng.uniform(-40.0, 40.0, size=count)
+    t0 = time.time()
+    pencils = [make_pencil(16, int((n - 16) // 16), 16, seed=1000 + i) for i, n in enumerate(ns)]
+    gen = time.time() - t0
+    out, wall = jdqz_batch(pencils, [complex(3.0, s) for s in sig], k=16, tol=1e-10,
+                           maxiter=maxiter, maxsub=80, minsub=32, precision=precision,
+                           threads=threads)
+    pairs = sum(o[2]["nconv"] for o in out)
+    slow = max(o[2]["seconds"] for o in out)
+    print(f"sweep count={count} threads={threads} precision={precision} gen={gen:.1f}s "
+          f"wall={wall:.2f}s pairs={pairs} eigenpairs/s={pairs / wall:.2f} slowest_solve={slow:.2f}s "
+          f"iters={[o[2]['iters'] for o in out]}")
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
+    ap.add_argument("--sweep", type=int, default=0, help="run the batched sweep of this many pencils")
+    ap.add_argument("--threads", type=int, default=16)
+    ap.add_argument("--maxiter", type=int, default=2000)
     ap.add_argument("--b", type=int, default=32)
     ap.add_argument("--nblk", type=int, default=31250)
     ap.add_argument("--t", type=int, default=64)
@@ -29,6 +55,8 @@ def main(argv=None):
     ap.add_argument("--projected", default="auto")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     a = ap.parse_args(argv)
+    if a.sweep:
+        return sweep(a.sweep, a.threads, a.precision, a.maxiter)
     P = make_pencil(a.b, a.nblk, a.t, seed=0)
     dev = DevicePencil(P)
     pc = DevicePreconditioner(dev, 3.0, "exact", precision=a.precision)
