@@ -5,8 +5,9 @@
 is loaded on first use; without it every solver call raises (there is no CPU
 compute path).
 """
-from .bbjd import DevicePencil, DevicePreconditioner, jdqz, jdqz_batch, jdqz_c  # noqa: F401
+from .bbjd import (DevicePencil, DevicePreconditioner, SparseLU, jdqz, jdqz_batch,  # noqa: F401
+                   jdqz_c)
 from .pencils import BBTPencil, make_pencil, start_vector  # noqa: F401
 
-__all__ = ["jdqz", "jdqz_batch", "jdqz_c", "DevicePencil", "DevicePreconditioner", "BBTPencil",
+__all__ = ["jdqz", "jdqz_batch", "jdqz_c", "DevicePencil", "DevicePreconditioner", "SparseLU", "BBTPencil",
            "make_pencil", "start_vector"]

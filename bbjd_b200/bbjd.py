@@ -125,6 +125,55 @@ class DevicePreconditioner:
             pass
 
 
+class SparseLU:
+    """Device LU of a block-bordered sparse matrix, in the place of the
+    sparse LU the reference's users build for ``A - sigma B`` (reference
+    README.md:40-44: ``SparseLU(M, colamd=True, pin_dense_rows=True)``).
+
+    ``M`` (scipy sparse or dense) must have the block-bordered form
+    (:func:`bbjd_b200.structure.detect`); it is packed, uploaded and
+    factored once by the device block-bordered LU, which needs no fill-
+    reducing ordering and keeps the dense tau rows in a t x t Schur
+    complement, so ``colamd`` and ``pin_dense_rows`` are accepted for
+    compatibility and have no effect.  ``solve(b)`` takes and returns host
+    arrays; passed as ``jdqz``'s preconditioner with a block-bordered
+    ``A, B`` the factors are applied on the device directly.
+    """
+
+    def __init__(self, M, colamd: bool = True, pin_dense_rows: bool = True,
+                 precision: str = "fp64"):
+        from .structure import matrix_from_sparse
+        P = matrix_from_sparse(M)
+        if P is None:
+            raise ValueError("SparseLU: M does not have the block-bordered form (block-"
+                             "tridiagonal interior with b in (8, 16, 32), at most 128 tau rows)")
+        self.b, self.t, self.n = P.b, P.t, P.n
+        self.shape = (P.n, P.n)
+        self._dev = DevicePencil(P)
+        self.device = DevicePreconditioner(self._dev, 0.0, "exact", precision=precision)
+
+    def solve(self, rhs) -> np.ndarray:
+        import torch
+        x = np.asarray(rhs, dtype=np.complex128)
+        if x.shape[0] != self.n or x.ndim not in (1, 2):
+            raise ValueError(f"rhs must have shape ({self.n},) or ({self.n}, m); got {x.shape}")
+        cols = x.reshape(self.n, -1)
+        xd = torch.from_numpy(np.ascontiguousarray(cols.T)).to("cuda")
+        yd = torch.empty_like(xd)
+        lib = self.device._lib
+        for j in range(xd.shape[0]):
+            st = lib.bbjd_precond_solve(self.device.handle, 1, xd[j].data_ptr(), yd[j].data_ptr(),
+                                        torch.cuda.current_stream().cuda_stream)
+            if st != 0:
+                raise RuntimeError(f"bbjd_precond_solve failed: {_lib.STATUS_MSG.get(st, st)}")
+        y = yd.cpu().numpy().T
+        return y.reshape(x.shape).copy()
+
+    def close(self):
+        self.device.close()
+        self._dev.close()
+
+
 def _raise_status(status: int, nconv: int, k: int, iters: int, verbose: int):
     """Status mapping of reference bbjd.py:248-266."""
     if status < 0:
@@ -135,14 +184,21 @@ def _raise_status(status: int, nconv: int, k: int, iters: int, verbose: int):
                       RuntimeWarning, stacklevel=3)
 
 
-def _marshal(res: _lib.Result, n: int):
+def _marshal(res: _lib.Result, n: int, row_major: bool = False):
+    """Copy a bbjd_result out before bbjd_result_free.  ``row_major``: the
+    device already wrote the (n, nconv) row-major array (BBJD_EVEC_ROW_MAJOR),
+    so the copy is contiguous; otherwise the n x nconv column-major vectors
+    are transposed on the host as in the reference (_bbjd_c.c:240-246)."""
     nconv = int(res.nconv)
     if nconv > 0:
         ev = np.ctypeslib.as_array(C.cast(res.eigenvalues, C.POINTER(C.c_double)),
                                    shape=(2 * nconv,)).view(np.complex128).copy()
         vecs = np.ctypeslib.as_array(C.cast(res.eigenvectors, C.POINTER(C.c_double)),
                                      shape=(2 * n * nconv,)).view(np.complex128)
-        evecs = np.array(vecs.reshape(nconv, n).T)      # (n, nconv), C order
+        if row_major:
+            evecs = vecs.reshape(n, nconv).copy()
+        else:
+            evecs = np.array(vecs.reshape(nconv, n).T)      # (n, nconv), C order
         resid = np.ctypeslib.as_array(res.residuals, shape=(nconv,)).copy()
     else:
         ev = np.zeros(0, np.complex128)
@@ -258,6 +314,7 @@ def _solve_device(dev: DevicePencil, pc, k, sigma, target, tol, maxiter, maxsub,
     if lock not in _LOCK:
         raise ValueError(f"lock must be one of {list(_LOCK)}")
     ext.lock_rule = _LOCK[lock]
+    ext.evec_layout = 1        # BBJD_EVEC_ROW_MAJOR: the (n, nconv) array comes back ready
     ws = lib.bbjd_workspace_alloc(C.byref(p))
     if not ws:
         raise MemoryError("bbjd_workspace_alloc failed (device memory)")
@@ -268,7 +325,7 @@ def _solve_device(dev: DevicePencil, pc, k, sigma, target, tol, maxiter, maxsub,
     finally:
         lib.bbjd_workspace_free(ws)
     try:
-        ev, evecs, resid = _marshal(res, n)
+        ev, evecs, resid = _marshal(res, n, row_major=True)
     finally:
         lib.bbjd_result_free(C.byref(res))
     stats = {
@@ -366,6 +423,25 @@ def jdqz(
             return ev, evecs, {"nconv": nconv, "iters": iters, "status": status,
                                "residuals": resid, "device": stats}
         return ev, evecs
+
+    # ---- sparse block-bordered pencil: packed and solved on the device ----
+    device_pc = (preconditioner is None or isinstance(preconditioner, (str, SparseLU,
+                                                                         DevicePreconditioner)))
+    if device_pc and (sp.issparse(A) or isinstance(A, np.ndarray)) and \
+            (B is None or sp.issparse(B) or isinstance(B, np.ndarray)):
+        from .structure import pencil_from_sparse
+        P = pencil_from_sparse(A, B, b_is_identity=B is None)
+        if P is not None:
+            pc = preconditioner.device if isinstance(preconditioner, SparseLU) else preconditioner
+            if pc is not None and not isinstance(pc, str) and pc.n != P.n:
+                raise ValueError(f"preconditioner has size {pc.n}; the pencil has {P.n}")
+            return jdqz(P, None, k=k, sigma=sigma, which=which, tol=tol, maxiter=maxiter,
+                        maxsub=maxsub, minsub=minsub, inner_maxiter=inner_maxiter,
+                        inner_tol=inner_tol, preconditioner=pc, v0=v0, verbose=verbose,
+                        return_info=return_info, timing=timing, projected=projected,
+                        lock=lock, precision=precision)
+        if isinstance(preconditioner, (str, SparseLU, DevicePreconditioner)):
+            raise ValueError("a device preconditioner needs a block-bordered A, B pencil")
 
     # ---- callback path: validation as reference bbjd.py:160-224 ----
     if isinstance(A, np.ndarray):
@@ -469,6 +545,7 @@ def jdqz_batch(pencils, sigmas, k: int = 6, tol: float = 1e-10, maxiter: int = 2
         exts[i].precision = 1 if precision == "mixed" else 0
         exts[i].projected = _PROJECTED[projected]
         exts[i].lock_rule = _LOCK[lock]
+        exts[i].evec_layout = 1
         wss[i] = lib.bbjd_workspace_alloc(C.byref(p))
         if not wss[i]:
             for j in range(i):
@@ -488,7 +565,7 @@ def jdqz_batch(pencils, sigmas, k: int = 6, tol: float = 1e-10, maxiter: int = 2
     out = []
     for i, d in enumerate(devs):
         try:
-            ev, evecs, resid = _marshal(results[i], d.n)
+            ev, evecs, resid = _marshal(results[i], d.n, row_major=True)
         finally:
             lib.bbjd_result_free(C.byref(results[i]))
         out.append((ev, evecs, {"nconv": int(results[i].nconv), "iters": int(results[i].iters),

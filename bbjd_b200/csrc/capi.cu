@@ -3,11 +3,13 @@
 #include "engine.cuh"
 
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <new>
 #include <thread>
 #include <atomic>
+#include <mutex>
 
 namespace bbjd {
 
@@ -126,6 +128,35 @@ static bool params_ok(const bbjd_params *p, const bbjd_workspace *ws) {
            ws->nev >= p->nev && p->tol > 0 && p->maxiter >= 0;
 }
 
+extern "C" int scipy_openblas_get_num_threads(void);
+extern "C" void scipy_openblas_set_num_threads(int);
+
+// The k x k projected solves (k <= a few hundred) run fastest on one BLAS
+// thread: at these sizes the pool's fork/join costs more than it saves
+// (ZHSEQR at k = 140: 11.7 ms on 1 thread, 13.4 ms on 8).  While a device
+// solve runs, the LAPACK library the engine links is held at one thread;
+// the caller's setting comes back when the last concurrent solve returns.
+// Callback-mode solves leave it alone, since the caller's own host code
+// runs inside them.
+class BlasOneThread {
+public:
+    BlasOneThread() {
+        std::lock_guard<std::mutex> g(mu());
+        if (users()++ == 0) {
+            saved() = scipy_openblas_get_num_threads();
+            scipy_openblas_set_num_threads(1);
+        }
+    }
+    ~BlasOneThread() {
+        std::lock_guard<std::mutex> g(mu());
+        if (--users() == 0) scipy_openblas_set_num_threads(saved());
+    }
+private:
+    static std::mutex &mu() { static std::mutex m; return m; }
+    static int &users() { static int u = 0; return u; }
+    static int &saved() { static int v = 1; return v; }
+};
+
 // Runs one engine solve; fills the extension's instrumentation.
 static bbjd_status run_engine(const bbjd_params *p, bbjd_workspace *ws, bbjd_result *r,
                               bbjd_device_ext *ext, Operators *ops, Engine &E, cudaStream_t st,
@@ -134,6 +165,14 @@ static bbjd_status run_engine(const bbjd_params *p, bbjd_workspace *ws, bbjd_res
     const long long l0 = g_launches.load();
     bbjd_status s = E.init(p, ws, r, ext, ops, st);
     if (s == BBJD_SUCCESS) s = E.run();
+    if (p->verbose >= 1 && E.proj_mode == BBJD_PROJ_SCHUR)
+        fprintf(stderr, "  projected solve %.3f s: form H %.3f, Hessenberg %.3f, eigenvalues %.3f, "
+                "target vector %.3f, restart Schur form + reorder %.3f\n", E.qz_seconds, E.qz_split[0],
+                E.qz_split[1], E.qz_split[2], E.qz_split[3], E.qz_split[4]);
+    if (s != BBJD_ERR_CUDA && !(cb_failed && *cb_failed)) {
+        const bbjd_status f = E.finish_eigenvectors();
+        if (f != BBJD_SUCCESS) s = f;
+    }
     if (s == BBJD_ERR_CUDA || (cb_failed && *cb_failed)) {
         if (cb_failed && *cb_failed) s = BBJD_ERR_CALLBACK;
         r->status = s;
@@ -312,7 +351,10 @@ bbjd_status bbjd_solve_device(const bbjd_params *params, bbjd_device_ext *ext,
     Engine E;
     Operators *ops = make_device_ops(m, pc, &E.S, st);
     if (!ops) return result->status = BBJD_ERR_ALLOC;
-    s = run_engine(params, ws, result, ext, ops, E, st, nullptr);
+    {
+        BlasOneThread one;
+        s = run_engine(params, ws, result, ext, ops, E, st, nullptr);
+    }
     delete ops;
     if (own) cudaStreamDestroy(st);
     return s;

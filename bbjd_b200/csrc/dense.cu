@@ -523,6 +523,39 @@ bbjd_status gram(Scratch &S, int keep, const cplx *X, const cplx *Y, int64_t ldx
 }
 
 // ---------------------------------------------------------------------------
+// out (rows x ncols row-major, row stride ncols) = rows [r0, r0+rows) of Q
+// (column-major, ld).  32 x 32 tiles staged through shared memory, so both
+// the column reads and the row writes are coalesced; the +1 pad keeps the
+// transposed reads of the tile free of bank conflicts.
+__global__ void k_to_row_major(int64_t r0, int64_t rows, int ncols, int64_t ld,
+                               const cplx *__restrict__ Q, cplx *__restrict__ out) {
+    __shared__ cplx tile[32][33];
+    const int64_t i0 = (int64_t)blockIdx.x * 32;
+    const int j0 = blockIdx.y * 32;
+    const int tx = threadIdx.x, ty = threadIdx.y;      // 32 x 8 threads
+    for (int c = ty; c < 32; c += 8) {
+        const int64_t i = i0 + tx;
+        const int j = j0 + c;
+        if (i < rows && j < ncols) tile[c][tx] = Q[(int64_t)j * ld + r0 + i];
+    }
+    __syncthreads();
+    for (int r = ty; r < 32; r += 8) {
+        const int64_t i = i0 + r;
+        const int j = j0 + tx;
+        if (i < rows && j < ncols) out[i * ncols + j] = tile[tx][r];
+    }
+}
+
+bbjd_status to_row_major(int64_t r0, int64_t rows, int ncols, int64_t ld, const cplx *Q, cplx *out,
+                         cudaStream_t st) {
+    if (rows <= 0 || ncols <= 0) return BBJD_SUCCESS;
+    const dim3 grid((unsigned)((rows + 31) / 32), (unsigned)((ncols + 31) / 32)), block(32, 8);
+    k_to_row_major<<<grid, block, 0, st>>>(r0, rows, ncols, ld, Q, out);
+    BBJD_LAUNCH_CHECK();
+    return BBJD_SUCCESS;
+}
+
+// ---------------------------------------------------------------------------
 // Mixed-precision helpers: complex64 copies and passes over a complex64 basis.
 __global__ void k_cvt_c64(int64_t count, const double2 *__restrict__ in, float2 *__restrict__ out) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;

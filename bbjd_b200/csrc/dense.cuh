@@ -56,6 +56,10 @@ bbjd_status reduce_partials(const cplx *partial, int G, int X, cplx *out, cudaSt
 bbjd_status gram(Scratch &S, int keep, const cplx *X, const cplx *Y, int64_t ldx, cplx *partial,
                  int Gg, cplx *out, cudaStream_t st);
 
+// out (rows x ncols, row-major) = rows [r0, r0+rows) of the column-major Q.
+bbjd_status to_row_major(int64_t r0, int64_t rows, int ncols, int64_t ld, const cplx *Q, cplx *out,
+                         cudaStream_t st);
+
 // Mixed precision: out = complex64(in); the first CGS pass over a complex64
 // basis (dots into out[0:ncols], ||v||^2 into out[ncols]; v -= Q h).
 bbjd_status to_c64(int64_t count, const cplx *in, float2 *out, cudaStream_t st);

@@ -81,6 +81,8 @@ struct Engine {
     int *dflag = nullptr;      // device flags
     bool mixed = false;        // BBJD_MIXED: complex64 shadow of V for the first CGS pass
     float2 *Vs = nullptr;      // n x maxsub complex64 copy of V (ld n)
+    int evec_layout = BBJD_EVEC_COLUMN_MAJOR;
+    cplx *evd = nullptr;       // BBJD_EVEC_ROW_MAJOR: converged vectors, n x nev (ld n)
     cplx *pin = nullptr;       // pinned host staging for small results
     double *pin_d = nullptr;
     int *pin_i = nullptr;
@@ -93,9 +95,13 @@ struct Engine {
     // H = C^-1 MB = Q T Q^H (ld = maxsub); omega = eig(H)
     int proj_mode = BBJD_PROJ_QZ;
     bool schur_step = false;          // the last projected solve used the Schur form
-    std::vector<zc> hC, hT, hQ, tau, omega;
+    bool ritz_ready = false;          // hx holds the target's coefficients already
+    std::vector<zc> hC, hT, hx, tau, omega;
     std::vector<int> ipiv;
     double qz_seconds = 0;
+    // host seconds of the Schur-form projected solve: forming H, Hessenberg
+    // reduction, eigenvalues (QR), target vector, restart Schur form + reorder
+    double qz_split[5] = {0, 0, 0, 0, 0};
     long long dgks = 0, restarts = 0, duplicates = 0;
     double bytes_dev = 0;
     // locked eigenvalues and the window within which a Ritz value matches one
@@ -123,9 +129,11 @@ struct Engine {
     bbjd_status gmres(int ndefl, zc ta, zc tb, const cplx *r, cplx *z);
     int solve_projected(int k, int locked, int nkeep, int *target_pos);
     int solve_projected_schur(int k, int nkeep, bool reorder, int *target_pos);
+    void hessenberg_eigvec(int k, zc w, zc *x);
     void select_and_scan(int k, int nkeep, int *target_pos);
     void ritz_coefficients(int k, int p, zc ta, zc tb, cplx *x);
     bbjd_status sync();
+    bbjd_status finish_eigenvectors();
     void second_pass_bytes(int cls, int k);
 };
 

@@ -27,6 +27,9 @@ void scipy_ztgsen_(const int *ijob, const int *wantq, const int *wantz, const in
                    bbjd_zomplex *z, const int *ldz, int *m, double *pl, double *pr, double *dif,
                    bbjd_zomplex *work, const int *lwork, int *iwork, const int *liwork, int *info);
 void scipy_zgetrf_(const int *m, const int *n, bbjd_zomplex *a, const int *lda, int *ipiv, int *info);
+void scipy_ztrtrs_(const char *uplo, const char *trans, const char *diag, const int *n,
+                   const int *nrhs, const bbjd_zomplex *a, const int *lda, bbjd_zomplex *b,
+                   const int *ldb, int *info);
 void scipy_zgetrs_(const char *trans, const int *n, const int *nrhs, const bbjd_zomplex *a,
                    const int *lda, const int *ipiv, bbjd_zomplex *b, const int *ldb, int *info);
 void scipy_zgehrd_(const int *n, const int *ilo, const int *ihi, bbjd_zomplex *a, const int *lda,
@@ -138,6 +141,8 @@ bbjd_status Engine::init(const bbjd_params *p, bbjd_workspace *w, bbjd_result *r
     BBJD_CUDA_TRY(cudaMemset(dflag, 0, sizeof(int) * FL_N));
     mixed = e && e->precision == BBJD_MIXED;
     if (mixed) BBJD_CUDA_TRY(cudaMalloc(&Vs, sizeof(float2) * (size_t)n * maxsub));
+    evec_layout = e ? e->evec_layout : BBJD_EVEC_COLUMN_MAJOR;
+    if (evec_layout == BBJD_EVEC_ROW_MAJOR) BBJD_CUDA_TRY(cudaMalloc(&evd, nv * (size_t)nev));
     const size_t pin_c = 8 * (size_t)(maxsub + nev + 8);
     BBJD_CUDA_TRY(cudaMallocHost(&pin, sizeof(cplx) * pin_c));
     BBJD_CUDA_TRY(cudaMallocHost(&pin_d, sizeof(double) * 16));
@@ -148,6 +153,8 @@ bbjd_status Engine::init(const bbjd_params *p, bbjd_workspace *w, bbjd_result *r
     bwork.resize(maxsub);
     sel.resize(maxsub);
     hC.resize((size_t)maxsub * maxsub);
+    hT.resize((size_t)maxsub * maxsub);
+    hx.resize(maxsub);
     tau.resize(maxsub);
     omega.resize(maxsub);
     ipiv.resize(maxsub);
@@ -164,6 +171,8 @@ void Engine::release() {
     cudaFree(dscal); cudaFree(dflag);
     cudaFree(Vs);
     Vs = nullptr;
+    cudaFree(evd);
+    evd = nullptr;
     cudaFreeHost(pin); cudaFreeHost(pin_d); cudaFreeHost(pin_i);
     if (own_stream && st) cudaStreamDestroy(st);
     st = nullptr;
@@ -174,6 +183,24 @@ void Engine::second_pass_bytes(int cls, int k) {
     const double b = 16.0 * (double)n * (2.0 * k + 3.0);
     T.bytes[cls] += b;
     bytes_dev += b;
+}
+
+// BBJD_EVEC_ROW_MAJOR: write the converged vectors to the host result as the
+// (n, nconv) row-major array, transposed on the device in row chunks of at
+// most n elements (staged through g1) so the host does no strided copy.
+bbjd_status Engine::finish_eigenvectors() {
+    const int nc = (int)res->nconv;
+    if (!evd || nc == 0) return BBJD_SUCCESS;
+    const int64_t rows = std::max<int64_t>(1, n / nc);
+    for (int64_t r0 = 0; r0 < n; r0 += rows) {
+        const int64_t rr = std::min<int64_t>(rows, n - r0);
+        bbjd_status s = to_row_major(r0, rr, nc, n, evd, g1, st);
+        if (s) return s;
+        BBJD_CUDA_TRY(cudaMemcpyAsync(res->eigenvectors + (size_t)r0 * nc, g1, sizeof(cplx) * rr * nc,
+                                      cudaMemcpyDeviceToHost, st));
+        BBJD_CUDA_TRY(cudaStreamSynchronize(st));
+    }
+    return BBJD_SUCCESS;
 }
 
 bbjd_status Engine::sync() {
@@ -294,6 +321,7 @@ static double target_value(zc lam, zc sigma, int target) {
 // workspace's host MA, MB (ld = maxsub).  Returns 0 or -1 on a LAPACK error.
 int Engine::solve_projected(int k, int locked, int nkeep, int *target_pos) {
     (void)locked;
+    ritz_ready = false;
     auto t0 = std::chrono::steady_clock::now();
     const int bk = k, lda = (int)maxsub;
     zc *MA = ws->MA, *MB = ws->MB, *SA = ws->SA, *SB = ws->SB, *ZA = ws->ZA, *ZB = ws->ZB;
@@ -383,24 +411,73 @@ void Engine::select_and_scan(int k, int nkeep, int *target_pos) {
 // error, 0 on success.
 int Engine::solve_projected_schur(int k, int nkeep, bool reorder, int *target_pos) {
     auto t0 = std::chrono::steady_clock::now();
+    ritz_ready = false;
     const int bk = k, ld = (int)maxsub, one = 1;
     int info = 0;
     zc *MA = ws->MA, *MB = ws->MB;
     zc *T = ws->SA, *Q = ws->ZB;
+    double c_all = 0.0, c_low = 0.0;
     for (int j = 0; j < k; ++j)
         for (int i = 0; i < k; ++i) {
             const size_t e = i + (size_t)j * maxsub;
             hC[e] = nu0 * MA[e] + mu0 * MB[e];
             T[e] = MB[e];
+            const double a2 = std::norm(hC[e]);
+            c_all += a2;
+            if (i > j) c_low += a2;
         }
-    scipy_zgetrf_(&bk, &bk, hC.data(), &ld, ipiv.data(), &info);
-    if (info > 0) return 1;
-    if (info < 0) return -1;
-    scipy_zgetrs_("N", &bk, &bk, hC.data(), &ld, ipiv.data(), T, &ld, &info);
-    if (info) return -1;
+    // W is built column by column as the orthonormal basis of
+    // (nu0 A + mu0 B) V (each new w orthogonalised against the earlier
+    // columns and the locked Q_left), so C = W^H (nu0 A + mu0 B) V is upper
+    // triangular up to rounding and one triangular solve gives H.  Should the
+    // part below the diagonal exceed 1e-14 of ||C||_F, LU with pivoting.
+    if (c_low <= 1e-28 * c_all) {
+        scipy_ztrtrs_("U", "N", "N", &bk, &bk, hC.data(), &ld, T, &ld, &info);
+        if (info > 0) return 1;
+        if (info < 0) return -1;
+    } else {
+        scipy_zgetrf_(&bk, &bk, hC.data(), &ld, ipiv.data(), &info);
+        if (info > 0) return 1;
+        if (info < 0) return -1;
+        scipy_zgetrs_("N", &bk, &bk, hC.data(), &ld, ipiv.data(), T, &ld, &info);
+        if (info) return -1;
+    }
+    auto t1 = std::chrono::steady_clock::now();
     const int lw = (int)zwork.size();
     scipy_zgehrd_(&bk, &one, &bk, T, &ld, tau.data(), zwork.data(), &lw, &info);
     if (info) return -1;
+    auto t2 = std::chrono::steady_clock::now();
+    qz_split[0] += std::chrono::duration<double>(t1 - t0).count();
+    qz_split[1] += std::chrono::duration<double>(t2 - t1).count();
+    auto to_lambda = [&](int i) {
+        const zc w = omega[i];
+        if (std::abs(w) < 1e-300 * std::abs(nu0)) { alpha[i] = 1.0; beta[i] = 0.0; return; }
+        alpha[i] = (1.0 / w - mu0) / nu0;
+        beta[i] = 1.0;
+    };
+    if (!reorder) {
+        // Between restarts only the eigenvalues and the target's eigenvector
+        // are used, so the QR iteration runs without accumulating Schur
+        // vectors (the Schur form itself is needed only to restart); the
+        // eigenvector comes from inverse iteration on the Hessenberg form.
+        zc *Hh = hC.data();
+        for (int j = 0; j < k; ++j)
+            for (int i = 0; i < k; ++i)
+                Hh[i + (size_t)j * maxsub] = i <= j + 1 ? T[i + (size_t)j * maxsub] : zc(0.0);
+        scipy_zhseqr_("E", "N", &bk, &one, &bk, Hh, &ld, omega.data(), Q, &ld, zwork.data(), &lw, &info);
+        if (info) return -1;
+        auto t3 = std::chrono::steady_clock::now();
+        for (int i = 0; i < k; ++i) to_lambda(i);
+        select_and_scan(k, 0, target_pos);
+        hessenberg_eigvec(k, omega[*target_pos], hx.data());
+        ritz_ready = true;
+        schur_step = true;
+        auto t4 = std::chrono::steady_clock::now();
+        qz_split[2] += std::chrono::duration<double>(t3 - t2).count();
+        qz_split[3] += std::chrono::duration<double>(t4 - t3).count();
+        qz_seconds += std::chrono::duration<double>(t4 - t0).count();
+        return 0;
+    }
     for (int j = 0; j < k; ++j) memcpy(Q + (size_t)j * maxsub, T + (size_t)j * maxsub, sizeof(zc) * k);
     scipy_zunghr_(&bk, &one, &bk, Q, &ld, tau.data(), zwork.data(), &lw, &info);
     if (info) return -1;
@@ -411,12 +488,6 @@ int Engine::solve_projected_schur(int k, int nkeep, bool reorder, int *target_po
     if (info) return -1;
     for (int j = 0; j < k; ++j)
         for (int i = j + 1; i < k; ++i) T[i + (size_t)j * maxsub] = 0.0;
-    auto to_lambda = [&](int i) {
-        const zc w = omega[i];
-        if (std::abs(w) < 1e-300 * std::abs(nu0)) { alpha[i] = 1.0; beta[i] = 0.0; return; }
-        alpha[i] = (1.0 / w - mu0) / nu0;
-        beta[i] = 1.0;
-    };
     for (int i = 0; i < k; ++i) to_lambda(i);
     if (reorder) {
         select_and_scan(k, nkeep, nullptr);
@@ -429,7 +500,9 @@ int Engine::solve_projected_schur(int k, int nkeep, bool reorder, int *target_po
     }
     select_and_scan(k, 0, target_pos);
     schur_step = true;
-    qz_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    const auto t5 = std::chrono::steady_clock::now();
+    qz_split[4] += std::chrono::duration<double>(t5 - t2).count();
+    qz_seconds += std::chrono::duration<double>(t5 - t0).count();
     return 0;
 }
 
@@ -438,6 +511,10 @@ int Engine::solve_projected_schur(int k, int nkeep, bool reorder, int *target_po
 // of (tb SA - ta SB) with y[p] = 1 (QZ form), or of (T - omega_p I) in the
 // harmonic Schur form.
 void Engine::ritz_coefficients(int k, int p, zc ta, zc tb, cplx *x) {
+    if (ritz_ready) {
+        for (int i = 0; i < k; ++i) x[i] = C(hx[i]);
+        return;
+    }
     std::vector<zc> y(p + 1);
     y[p] = 1.0;
     const zc *SA = ws->SA, *SB = ws->SB, *ZB = ws->ZB;
@@ -458,6 +535,71 @@ void Engine::ritz_coefficients(int k, int p, zc ta, zc tb, cplx *x) {
         zc acc = 0.0;
         for (int j = 0; j <= p; ++j) acc += ZB[i + (size_t)j * maxsub] * y[j];
         x[i] = C(acc);
+    }
+}
+
+// Eigenvector x of H = Q Hh Q^H for its eigenvalue w, where ZGEHRD left the
+// Hessenberg matrix Hh in the upper part of T (= ws->SA, ld maxsub) and the
+// Householder vectors of Q below its subdiagonal (scalars in tau).  Two
+// steps of inverse iteration on Hh - w I: an LU factorisation with partial
+// pivoting between adjacent rows (O(k^2) for a Hessenberg matrix), pivots
+// below eps * ||Hh||_1 raised to that size so the near-singular solve stays
+// finite, a first solve U y = (1, ..., 1) and a second full solve of y.
+// Then x = Q y applies the reflectors H(k-2), ..., H(0) in that order.
+// x is unnormalised: the Ritz vector V x is normalised on the device.
+void Engine::hessenberg_eigvec(int k, zc w, zc *x) {
+    const size_t ld = maxsub;
+    const zc *Tm = ws->SA;
+    zc *U = hT.data();
+    double hnorm = 0.0;
+    for (int j = 0; j < k; ++j) {
+        double c = 0.0;
+        for (int i = 0; i <= std::min(j + 1, k - 1); ++i) c += std::abs(Tm[i + j * ld]);
+        hnorm = std::max(hnorm, c);
+    }
+    const double eps3 = std::max(hnorm, 1e-300) * DBL_EPSILON;
+    for (int j = 0; j < k; ++j)
+        for (int i = 0; i <= std::min(j + 1, k - 1); ++i)
+            U[i + j * ld] = Tm[i + j * ld] - (i == j ? w : zc(0.0));
+    std::vector<zc> mult(k);
+    std::vector<char> swapped(k, 0);
+    for (int j = 0; j + 1 < k; ++j) {
+        if (std::abs(U[j + 1 + j * ld]) > std::abs(U[j + j * ld])) {
+            swapped[j] = 1;
+            for (int c = j; c < k; ++c) std::swap(U[j + c * ld], U[j + 1 + c * ld]);
+        }
+        if (std::abs(U[j + j * ld]) < eps3) U[j + j * ld] = eps3;
+        const zc m = U[j + 1 + j * ld] / U[j + j * ld];
+        mult[j] = m;
+        for (int c = j + 1; c < k; ++c) U[j + 1 + c * ld] -= m * U[j + c * ld];
+        U[j + 1 + j * ld] = 0.0;
+    }
+    if (std::abs(U[(k - 1) + (k - 1) * ld]) < eps3) U[(k - 1) + (k - 1) * ld] = eps3;
+    auto back_solve = [&](zc *y) {
+        for (int i = k - 1; i >= 0; --i) {
+            zc acc = y[i];
+            for (int c = i + 1; c < k; ++c) acc -= U[i + c * ld] * y[c];
+            y[i] = acc / U[i + i * ld];
+            if (std::abs(y[i]) > 1e150)      // rescale before a run of tiny pivots overflows
+                for (int c = 0; c < k; ++c) y[c] *= 1e-150;
+        }
+        double nrm = 0.0;
+        for (int i = 0; i < k; ++i) nrm = std::max(nrm, std::abs(y[i]));
+        for (int i = 0; i < k; ++i) y[i] /= nrm;
+    };
+    for (int i = 0; i < k; ++i) x[i] = 1.0;
+    back_solve(x);
+    for (int j = 0; j + 1 < k; ++j) {
+        if (swapped[j]) std::swap(x[j], x[j + 1]);
+        x[j + 1] -= mult[j] * x[j];
+    }
+    back_solve(x);
+    for (int i = k - 2; i >= 0; --i) {
+        zc s = x[i + 1];
+        for (int r = i + 2; r < k; ++r) s += std::conj(Tm[r + i * ld]) * x[r];
+        s *= tau[i];
+        x[i + 1] -= s;
+        for (int r = i + 2; r < k; ++r) x[r] -= s * Tm[r + i * ld];
     }
 }
 
@@ -757,8 +899,12 @@ bbjd_status Engine::run() {
                                       ? std::max(tol * 100, lock_rel * std::max(1.0, std::abs(lam)))
                                       : tol * 100});
             res->eigenvalues[res->nconv] = lam;
-            BBJD_CUDA_TRY(cudaMemcpyAsync(res->eigenvectors + (size_t)res->nconv * n, u,
-                                          sizeof(cplx) * n, cudaMemcpyDeviceToHost, st));
+            if (evd)
+                BBJD_CUDA_TRY(cudaMemcpyAsync(evd + (size_t)res->nconv * n, u, sizeof(cplx) * n,
+                                              cudaMemcpyDeviceToDevice, st));
+            else
+                BBJD_CUDA_TRY(cudaMemcpyAsync(res->eigenvectors + (size_t)res->nconv * n, u,
+                                              sizeof(cplx) * n, cudaMemcpyDeviceToHost, st));
             res->residuals[res->nconv] = rel;
             res->nconv++;
             if (P->verbose >= 1)

@@ -2,12 +2,17 @@
 
     python -m bbjd_b200.profile [--b 32] [--nblk 31250] [--t 64] [--k 64]
                                 [--iters 30] [--maxsub 200] [--minsub 80]
+                                [--preconditioner exact|block_jacobi]
+                                [--inner-maxiter 0] [--inner-tol 1e-2]
+    python -m bbjd_b200.profile --sweep 32 [--threads 16] [--maxiter 2000]
 
-Builds the seeded pencil, uploads it, factors the exact LU of A - 3 B on the
-device, runs `iters` outer JDQZ iterations and prints the per-kernel-class
-CUDA-event times and algorithmic bandwidths.  The defaults are the
-n = 1,000,064 benchmark pencil; a smaller --nblk gives a case small enough
-for multi-pass ncu captures.
+Builds the seeded pencil, uploads it, factors the exact LU (or the block
+Jacobi preconditioner) of A - 3 B on the device, runs `iters` outer JDQZ
+iterations and prints the per-kernel-class CUDA-event times and algorithmic
+bandwidths.  The defaults are the n = 1,000,064 benchmark pencil; a smaller
+--nblk gives a case small enough for multi-pass ncu captures; with
+--inner-maxiter > 0 the correction equation is solved by GMRES.  --sweep N
+runs the batched sweep of N pencils instead (sweep() below).
 """
 from __future__ import annotations
 
@@ -54,15 +59,20 @@ def main(argv=None):
     ap.add_argument("--minsub", type=int, default=80)
     ap.add_argument("--projected", default="auto")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--preconditioner", default="exact", choices=["exact", "block_jacobi"])
+    ap.add_argument("--inner-maxiter", type=int, default=0)
+    ap.add_argument("--inner-tol", type=float, default=1e-2)
+    ap.add_argument("--verbose", type=int, default=0)
     a = ap.parse_args(argv)
     if a.sweep:
         return sweep(a.sweep, a.threads, a.precision, a.maxiter)
     P = make_pencil(a.b, a.nblk, a.t, seed=0)
     dev = DevicePencil(P)
-    pc = DevicePreconditioner(dev, 3.0, "exact", precision=a.precision)
+    pc = DevicePreconditioner(dev, 3.0, a.preconditioner, precision=a.precision)
     t0 = time.time()
     ev, _, info = jdqz(dev, k=a.k, sigma=3.0, tol=1e-10, maxiter=a.iters, maxsub=a.maxsub,
-                       minsub=a.minsub, preconditioner=pc, v0=start_vector(P.n, 1),
+                       minsub=a.minsub, inner_maxiter=a.inner_maxiter, inner_tol=a.inner_tol,
+                       preconditioner=pc, v0=start_vector(P.n, 1), verbose=a.verbose,
                        return_info=True, timing=True, projected=a.projected,
                        precision=a.precision)
     wall = time.time() - t0

@@ -55,6 +55,10 @@ enum { BBJD_PROJ_AUTO = 0, BBJD_PROJ_QZ = 1, BBJD_PROJ_SCHUR = 2 };
  *                         (reference jd_core.c:369, 439), which returns an
  *                         ill-conditioned eigenvalue many times over. */
 enum { BBJD_LOCK_ROBUST = 0, BBJD_LOCK_REFERENCE = 1 };
+
+/* Layout of result->eigenvectors from a device solve. */
+enum { BBJD_EVEC_COLUMN_MAJOR = 0, BBJD_EVEC_ROW_MAJOR = 1 };
+
 enum { BBJD_PC_NONE = 0, BBJD_PC_BBT_LU = 1, BBJD_PC_BLOCK_JACOBI = 2 };
 
 /* Copy a BBT pencil to the current device.  from_host = 1: pointers are host
@@ -98,6 +102,13 @@ typedef struct {
     int     lock_rule;          /* BBJD_LOCK_ROBUST (default) or _REFERENCE     */
     double  lock_rel;           /* relative lock window; 0 = 1e-6               */
     void   *stream;             /* cudaStream_t, NULL = a private stream        */
+    int     evec_layout;        /* BBJD_EVEC_COLUMN_MAJOR (default): n x nev
+                                   column-major, as bbjd_solve.
+                                   BBJD_EVEC_ROW_MAJOR: result->eigenvectors
+                                   holds the (n, nconv) row-major array a
+                                   Python caller returns, transposed on the
+                                   device at the end of the solve (saves the
+                                   host an O(n nconv) strided copy)          */
     /* out */
     double  seconds_total;      /* wall time of the solve                       */
     double  seconds_qz;         /* host projected QZ + reorder                  */
