@@ -45,9 +45,12 @@ WORKLOAD_NAME = "bbt_n1000064_k64"
 # pencil (same algorithm and start vector as the reference), used to turn
 # the reference's measured seconds per outer iteration into eigenpairs/s.
 PAIRS_PER_ITER = 13 / 2000   # measured: 13 pairs in the 2000-iteration cap (FP64, B200)
-# DRAM traffic (read + write bytes) per launch of the fused A,B product from
-# an ncu capture (profiles/), or None.
-SPMV_TRAFFIC_BYTES = 4.149e9   # profiles/kernels_bbt_n131136.md, scaled by n
+# DRAM traffic (read + write bytes) of each kernel class per call, from ncu
+# captures on B200 (profiles/): the fused A,B product per launch, and the
+# ratio of measured DRAM bytes to algorithmic bytes for the CGS classes
+# (all their launches over 250 outer iterations, selected by NVTX range).
+SPMV_TRAFFIC_BYTES = 4.117e9   # profiles/launch_list_bbt_n1000064.md: 321.11 GB / 78 launches
+TRAFFIC_RATIO = {"pencil": 2418.65 / 2422.01, "orth": 1602.48 / 1606.63}   # profiles/class_traffic_bbt_n1000064.md
 
 
 def _env_rank():
@@ -293,7 +296,9 @@ def run_ours(args):
         ach = per_launch_bytes / per_launch_s / 1e9
         roof = {"bound": "hbm", "kernel": dom[0], "achieved": round(ach, 1), "peak": peak,
                 "unit": "GB/s", "frac": round(ach / peak, 4), "peak_kind": peak_kind,
-                "traffic": SPMV_TRAFFIC_BYTES if dom[0] == "spmv" else None,
+                "traffic": (SPMV_TRAFFIC_BYTES if dom[0] == "spmv" else
+                            round(TRAFFIC_RATIO[dom[0]] * per_launch_bytes) if dom[0] in TRAFFIC_RATIO
+                            else None),
                 "algorithmic_bytes_per_launch": per_launch_bytes}
     kern = {k: {"ms": round(v["ms"], 2), "calls": v["calls"],
                 "GBps": round(v["bytes"] / max(v["ms"], 1e-9) / 1e6, 1)}
