@@ -41,9 +41,13 @@ __global__ void __launch_bounds__(256) k_bbt_spmv(
     const int hw = lane / BS, row = lane - hw * BS, base = hw * BS;
     const int64_t gw = (int64_t)blockIdx.x * 8 + warp, nw = (int64_t)gridDim.x * 8;
     const int64_t ngroups = (nblk + BPW - 1) / BPW;
-    cplx tacc[NQ];
+    // NQ = 0: t is a power of two below 32 and one load of F^T covers 32/t
+    // columns (lane = column offset * t + tau); otherwise lane = tau and NQ
+    // loads cover the t tau values of one column.
+    constexpr int NA = NQ > 0 ? NQ : 1;
+    cplx tacc[NA];
 #pragma unroll
-    for (int q = 0; q < NQ; ++q) tacc[q] = mk(0.0, 0.0);
+    for (int q = 0; q < NA; ++q) tacc[q] = mk(0.0, 0.0);
     double rn = 0.0;
 
     for (int64_t gi = gw; gi < ngroups; gi += nw) {
@@ -74,15 +78,30 @@ __global__ void __launch_bounds__(256) k_bbt_spmv(
             for (int tau = 0; tau < t; ++tau) cfma(a, ldg_stream(pe + (int64_t)tau * nb), xtail[tau]);
             // tau-row partial sums over the 32 columns of this group
             const int64_t col0 = gi * 32;
+            if constexpr (NQ == 0) {
+                // element (tau, col0 + c) with c = k * 32/t + lane / t sits at
+                // FT + col0 * t + 32 k + lane; columns past nb (last group) read
+                // the last interior column and meet x = 0
+                const int cpl = 32 / t, cc = lane / t;
+                const int64_t last = (nb - 1) * t + (lane - cc * t);
+                const cplx *pf = FT + col0 * t + lane;
+#pragma unroll 1
+                for (int k = 0; k < t; ++k) {
+                    const cplx xv = shfl(xc, k * cpl + cc);
+                    const int64_t off = col0 * t + 32 * k + lane;
+                    cfma(tacc[0], ldg_stream(off <= last ? pf + 32 * k : FT + last), xv);
+                }
+            } else {
 #pragma unroll 4
-            for (int c = 0; c < 32; ++c) {
-                const cplx xv = shfl(xc, c);
-                const int64_t col = min(col0 + c, nb - 1);
-                const cplx *pf = FT + col * t;
+                for (int c = 0; c < 32; ++c) {
+                    const cplx xv = shfl(xc, c);
+                    const int64_t col = min(col0 + c, nb - 1);
+                    const cplx *pf = FT + col * t;
 #pragma unroll
-                for (int q = 0; q < NQ; ++q) {
-                    const int tau = lane + 32 * q;
-                    if (tau < t) cfma(tacc[q], ldg_stream(pf + tau), xv);
+                    for (int q = 0; q < NQ; ++q) {
+                        const int tau = lane + 32 * q;
+                        if (tau < t) cfma(tacc[q], ldg_stream(pf + tau), xv);
+                    }
                 }
             }
         }
@@ -99,10 +118,20 @@ __global__ void __launch_bounds__(256) k_bbt_spmv(
         }
     }
     // CTA reduction of the tau partials (fixed order over warps)
+    if constexpr (NQ == 0) {
+        // lanes tau, tau + t, tau + 2t, ... hold the same tau row
+        cplx v = tacc[0];
+        for (int o = t; o < 32; o <<= 1) {
+            v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+            v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+        }
+        if (lane < t) wtau[warp * t + lane] = v;
+    } else {
 #pragma unroll
-    for (int q = 0; q < NQ; ++q) {
-        const int tau = lane + 32 * q;
-        if (tau < t) wtau[warp * t + tau] = tacc[q];
+        for (int q = 0; q < NQ; ++q) {
+            const int tau = lane + 32 * q;
+            if (tau < t) wtau[warp * t + tau] = tacc[q];
+        }
     }
     __shared__ double srn[8];
     rn = warp_sum(rn);
@@ -179,7 +208,9 @@ static bbjd_status launch_spmv(const bbjd_bbt_matrix *m, const BBTScratch *sc, c
     k_bbt_spmv<BS, NQ><<<sc->G, 256, smem, st>>>(m->nblk, m->t, m->nb, m->Ad, m->Al, m->Au, \
                                                  m->Bd, m->E, m->FT, x, yA, yB, ta, tb, r,  \
                                                  sc->tau_part, sc->rn_part)
-    if (nq <= 1) BBJD_SPMV(1);
+    const int t = m->t;
+    if (t > 0 && t < 32 && (t & (t - 1)) == 0) BBJD_SPMV(0);
+    else if (nq <= 1) BBJD_SPMV(1);
     else if (nq == 2) BBJD_SPMV(2);
     else if (nq <= 4) BBJD_SPMV(4);
     else return BBJD_ERR_INVALID;

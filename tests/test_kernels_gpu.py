@@ -29,7 +29,7 @@ def _rand(n, seed):
 
 
 SPMV_CASES = [(8, 64, 4), (16, 256, 8), (16, 33, 8), (32, 100, 64), (32, 7, 32), (16, 40, 0),
-              (8, 1, 3), (32, 31, 96)]
+              (8, 1, 3), (32, 31, 96), (16, 50, 16), (8, 21, 1), (32, 9, 2), (8, 3, 16)]
 
 
 @pytest.mark.parametrize("b,nblk,t", SPMV_CASES)
