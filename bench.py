@@ -31,6 +31,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -73,7 +74,10 @@ class ClockSampler:
     def __init__(self, index: int):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{index}.csv")
+        # the raw samples go to $BBJD_CLOCKS_DIR (default: the temp dir); the
+        # JSON line carries their summary
+        out = os.environ.get("BBJD_CLOCKS_DIR") or tempfile.gettempdir()
+        self.path = os.path.join(out, f"clocks_rank{index}.csv")
 
     def __enter__(self):
         os.makedirs(os.path.dirname(self.path), exist_ok=True)
@@ -215,7 +219,9 @@ def run_ours(args):
     torch.cuda.set_device(local)
     if world > 1:
         from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=1800),
+        # short enough that ranks waiting on a dead peer end with an error;
+        # one solve takes about 40 s, a step with warm-up about 4 minutes
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600),
                                 device_id=torch.device("cuda", local))
     w = WORKLOAD
     seed = rank
