@@ -294,7 +294,7 @@ __global__ void __launch_bounds__(256) k_bcr_even(
 template <int BS, int R, typename T>
 __device__ __forceinline__ void bmv_add(cplx (&acc)[R], const T *__restrict__ Mb, int row,
                                         const cplx (&v)[R], int base, double sign) {
-#pragma unroll 8
+#pragma unroll 16
     for (int c = 0; c < BS; ++c) {
         const cplx mv = ldm(Mb + c * BS + row);
 #pragma unroll
@@ -308,7 +308,7 @@ __device__ __forceinline__ void bmv_add(cplx (&acc)[R], const T *__restrict__ Mb
 
 // rhs_next[m/2] = rhs[m] - Alpha rhs[m-1] - Beta rhs[m+1] for even m.
 template <int BS, int R, typename T>
-__global__ void __launch_bounds__(256) k_bcr_fwd(int64_t N, const T *__restrict__ Alpha,
+__global__ void __launch_bounds__(256, 2) k_bcr_fwd(int64_t N, const T *__restrict__ Alpha,
                                                  const T *__restrict__ Beta,
                                                  const cplx *__restrict__ rhs, int64_t rs,
                                                  cplx *__restrict__ nxt, int64_t ns) {
@@ -358,7 +358,7 @@ __global__ void k_bcr_top(const T *__restrict__ Dinv, const cplx *__restrict__ r
 // Back substitution of one level: even m copy from the level above,
 // odd m: x = Dinv rhs - DinvLo x[m-1] - DinvUp x[m+1].
 template <int BS, int R, typename T>
-__global__ void __launch_bounds__(256) k_bcr_bwd(int64_t N, const T *__restrict__ Dinv,
+__global__ void __launch_bounds__(256, 2) k_bcr_bwd(int64_t N, const T *__restrict__ Dinv,
                                                  const T *__restrict__ DinvLo,
                                                  const T *__restrict__ DinvUp,
                                                  const cplx *__restrict__ rhs, int64_t rs,

@@ -23,7 +23,7 @@
 namespace bbjd {
 
 template <int BS, int NQ>
-__global__ void __launch_bounds__(256) k_bbt_spmv(
+__global__ void __launch_bounds__(256, 2) k_bbt_spmv(
     int64_t nblk, int t, int64_t nb, const cplx *__restrict__ Ad, const cplx *__restrict__ Al,
     const cplx *__restrict__ Au, const cplx *__restrict__ Bd, const cplx *__restrict__ E,
     const cplx *__restrict__ FT, const cplx *__restrict__ x, cplx *__restrict__ yA,
@@ -62,7 +62,7 @@ __global__ void __launch_bounds__(256) k_bbt_spmv(
         const cplx *pu = Au + jc * BB + row;
         const cplx *pb = Bd + jc * BB + row;
         cplx a = mk(0.0, 0.0), bacc = mk(0.0, 0.0);
-#pragma unroll 8
+#pragma unroll 4
         for (int c = 0; c < BS; ++c) {
             const cplx xcc = shfl(xc, base + c), xpc = shfl(xp, base + c), xnc = shfl(xn, base + c);
             const cplx md = ldg_stream(pd + c * BS), ml = ldg_stream(pl + c * BS);
