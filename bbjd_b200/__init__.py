@@ -6,8 +6,8 @@ is loaded on first use; without it every solver call raises (there is no CPU
 compute path).
 """
 from .bbjd import (DevicePencil, DevicePreconditioner, SparseLU, jdqz, jdqz_batch,  # noqa: F401
-                   jdqz_c)
+                   jdqz_c, jdqz_device)
 from .pencils import BBTPencil, make_pencil, start_vector  # noqa: F401
 
-__all__ = ["jdqz", "jdqz_batch", "jdqz_c", "DevicePencil", "DevicePreconditioner", "SparseLU", "BBTPencil",
+__all__ = ["jdqz", "jdqz_batch", "jdqz_c", "jdqz_device", "DevicePencil", "DevicePreconditioner", "SparseLU", "BBTPencil",
            "make_pencil", "start_vector"]

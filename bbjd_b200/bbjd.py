@@ -361,6 +361,7 @@ def jdqz(
     projected: str = "auto",
     lock: str = "robust",
     precision: str = "fp64",
+    oracle=None,
 ):
     """Jacobi-Davidson QZ for ``A x = lambda B x``, the eigenvalues nearest
     ``sigma`` first.  Parameters, defaults, returns and errors are those of
@@ -384,7 +385,10 @@ def jdqz(
     window, jd_core.c:369, 439).  ``precision='mixed'`` stores the device
     LU factors in complex64 and runs the first CGS pass against V over a
     complex64 copy of V (the second pass, DGKS, residuals, projected pencil
-    and QZ stay FP64).
+    and QZ stay FP64).  ``oracle``: reference eigenvalues (e.g. from an FP64
+    run or ARPACK); with ``return_info`` the info dict then holds
+    ``error_vs_oracle``, the largest distance from a returned eigenvalue to
+    its nearest oracle value.
     """
     if which not in _TARGET_MAP:
         raise ValueError(f"which must be one of {list(_TARGET_MAP.keys())}; got {which!r}")
@@ -420,8 +424,8 @@ def jdqz(
                 pc.close()
         _raise_status(status, nconv, k, iters, verbose)
         if return_info:
-            return ev, evecs, {"nconv": nconv, "iters": iters, "status": status,
-                               "residuals": resid, "device": stats}
+            return ev, evecs, _with_oracle({"nconv": nconv, "iters": iters, "status": status,
+                                            "residuals": resid, "device": stats}, ev, oracle)
         return ev, evecs
 
     # ---- sparse block-bordered pencil: packed and solved on the device ----
@@ -439,7 +443,7 @@ def jdqz(
                         maxsub=maxsub, minsub=minsub, inner_maxiter=inner_maxiter,
                         inner_tol=inner_tol, preconditioner=pc, v0=v0, verbose=verbose,
                         return_info=return_info, timing=timing, projected=projected,
-                        lock=lock, precision=precision)
+                        lock=lock, precision=precision, oracle=oracle)
         if isinstance(preconditioner, (str, SparseLU, DevicePreconditioner)):
             raise ValueError("a device preconditioner needs a block-bordered A, B pencil")
 
@@ -499,9 +503,26 @@ def jdqz(
         inner_maxiter=inner_maxiter, inner_tol=inner_tol, verbose=verbose, v0=v0)
     _raise_status(status, nconv, k, iters, verbose)
     if return_info:
-        return evals, evecs, {'nconv': nconv, 'iters': iters, 'status': status,
-                              'residuals': resid}
+        return evals, evecs, _with_oracle({'nconv': nconv, 'iters': iters, 'status': status,
+                                           'residuals': resid}, evals, oracle)
     return evals, evecs
+
+
+def _with_oracle(info: dict, ev, oracle) -> dict:
+    if oracle is not None:
+        ref = np.asarray(oracle, dtype=np.complex128).reshape(-1)
+        info["error_vs_oracle"] = (float(max(np.min(np.abs(ref - e)) for e in ev))
+                                   if len(ev) and len(ref) else float("nan"))
+    return info
+
+
+def jdqz_device(pencil, **kwargs):
+    """``jdqz`` on a block-bordered pencil already on the device or on the
+    host (:class:`DevicePencil` / :class:`BBTPencil`): the device path with
+    ``jdqz``'s keyword arguments, without the sparse-structure detection."""
+    if not isinstance(pencil, (BBTPencil, DevicePencil)):
+        raise TypeError("jdqz_device takes a BBTPencil or a DevicePencil")
+    return jdqz(pencil, None, **kwargs)
 
 
 def jdqz_batch(pencils, sigmas, k: int = 6, tol: float = 1e-10, maxiter: int = 200,

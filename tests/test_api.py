@@ -1,0 +1,17 @@
+"""Host-side API pieces that need no GPU."""
+import numpy as np
+import pytest
+
+from bbjd_b200 import jdqz_device
+from bbjd_b200.bbjd import _with_oracle
+
+
+def test_error_vs_oracle_is_the_largest_nearest_distance():
+    info = _with_oracle({}, np.array([1.0 + 1e-9j, 2.0]), [2.0 + 1e-7, 1.0, 5.0])
+    assert info["error_vs_oracle"] == pytest.approx(1e-7, rel=1e-6)
+    assert "error_vs_oracle" not in _with_oracle({}, np.array([1.0]), None)
+
+
+def test_jdqz_device_takes_only_pencils():
+    with pytest.raises(TypeError):
+        jdqz_device(np.eye(4), k=1)

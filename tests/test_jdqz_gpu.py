@@ -8,7 +8,8 @@ import numpy as np
 import pytest
 import scipy.sparse as sp
 
-from bbjd_b200 import DevicePencil, DevicePreconditioner, jdqz, make_pencil, start_vector
+from bbjd_b200 import (DevicePencil, DevicePreconditioner, jdqz, jdqz_device, make_pencil,
+                       start_vector)
 from tests.parity import EIG_ATOL, assert_no_duplicates, match_set
 
 pytestmark = pytest.mark.gpu
@@ -158,3 +159,16 @@ def test_batched_sweep_equals_one_at_a_time():
         A, B = P.to_csc("A"), P.to_csc("B")
         for lam, x in zip(bev, bvec.T):
             assert np.linalg.norm(A @ x - lam * (B @ x)) / np.linalg.norm(x) < 1e-8
+
+
+def test_jdqz_device_reports_error_vs_oracle():
+    g = _load("bbt_n516")
+    P = make_pencil(int(g["b"]), int(g["nblk"]), int(g["t"]), seed=int(g["seed"]))
+    ev, _, info = jdqz_device(P, k=int(g["k"]), sigma=complex(g["sigma"]), tol=1e-10,
+                              maxiter=int(g["maxiter"]), maxsub=int(g["maxsub"]),
+                              minsub=int(g["minsub"]), preconditioner="exact",
+                              v0=start_vector(P.n, int(g["seed"]) + 1), return_info=True,
+                              oracle=g["eigenvalues"])
+    assert info["nconv"] == int(g["k"])
+    assert info["error_vs_oracle"] == pytest.approx(match_set(ev, g["eigenvalues"]).max())
+    assert info["error_vs_oracle"] < EIG_ATOL
