@@ -31,6 +31,23 @@ def openblas() -> tuple[str, str]:
     return libdir, os.path.basename(cands[0])
 
 
+def torch_lib_dir() -> str | None:
+    """Directory of PyTorch's shared libraries (its bundled MKL, inside
+    libtorch_cpu.so, gives the engine a faster ZGEEV), found without
+    importing torch; None when torch is not installed."""
+    import importlib.util
+    spec = importlib.util.find_spec("torch")
+    if not spec or not spec.submodule_search_locations:
+        return None
+    d = os.path.join(list(spec.submodule_search_locations)[0], "lib")
+    return d if os.path.exists(os.path.join(d, "libtorch_cpu.so")) else None
+
+
+def defines() -> list[str]:
+    d = torch_lib_dir()
+    return [f'-DBBJD_TORCH_LIB="{d}"'] if d else []
+
+
 def sources() -> list[str]:
     return sorted(glob.glob(os.path.join(CSRC, "*.cu")))
 
@@ -42,7 +59,7 @@ def _digest() -> str:
         with open(p, "rb") as f:
             h.update(p.encode())
             h.update(f.read())
-    h.update(" ".join(ARCH).encode())
+    h.update(" ".join(ARCH + defines()).encode())
     return h.hexdigest()
 
 
@@ -58,14 +75,14 @@ def build(force: bool = False, verbose: bool = False) -> str:
     objs = []
     for src in sources():
         obj = os.path.join(OUT_DIR, os.path.basename(src) + ".o")
-        cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
+        cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", *defines(),
                "-I", os.path.join(ROOT, "include"), "-c", src, "-o", obj]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
             print(" ".join(cmd), file=sys.stderr)
         subprocess.run(cmd, check=True)
         objs.append(obj)
-    cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, f"-L{libdir}", f"-l:{blas}",
+    cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, f"-L{libdir}", f"-l:{blas}", "-ldl",
            "-Xlinker", f"-rpath={libdir}"]
     subprocess.run(cmd, check=True)
     with open(stamp, "w") as f:

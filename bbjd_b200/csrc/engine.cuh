@@ -130,6 +130,7 @@ struct Engine {
     int solve_projected(int k, int locked, int nkeep, int *target_pos);
     int solve_projected_schur(int k, int nkeep, bool reorder, int *target_pos);
     void hessenberg_eigvec(int k, zc w, zc *x);
+    void dense_eigvec(int k, zc w, zc *x);
     void select_and_scan(int k, int nkeep, int *target_pos);
     void ritz_coefficients(int k, int p, zc ta, zc tb, cplx *x);
     bbjd_status sync();
