@@ -50,7 +50,7 @@ PAIRS_PER_ITER = 13 / 2000   # measured: 13 pairs in the 2000-iteration cap (FP6
 # captures on B200 (profiles/): the fused A,B product per launch, and the
 # ratio of measured DRAM bytes to algorithmic bytes for the CGS classes
 # (all their launches over 250 outer iterations, selected by NVTX range).
-SPMV_TRAFFIC_BYTES = 4.117e9   # profiles/launch_list_bbt_n1000064.md: 321.11 GB / 78 launches
+SPMV_TRAFFIC_BYTES = 4.117e9   # profiles/launch_list_bbt_n1000064.md: 317.04 GB / 77 launches
 TRAFFIC_RATIO = {"pencil": 2418.65 / 2422.01, "orth": 1602.48 / 1606.63}   # profiles/class_traffic_bbt_n1000064.md
 
 
