@@ -8,6 +8,7 @@
 #include <cstring>
 #include <new>
 #include <thread>
+#include <algorithm>
 #include <atomic>
 #include <mutex>
 
@@ -373,20 +374,31 @@ bbjd_status bbjd_solve_batch(int count, const bbjd_params *params, bbjd_device_e
     }
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return BBJD_ERR_CUDA;
+    // Largest solves first (cost ~ n x maxiter x maxsub, known up front):
+    // the threads then finish close together instead of one long solve
+    // starting last.  Results stay at their input positions.
+    std::vector<int> order(count);
+    for (int i = 0; i < count; ++i) order[i] = i;
+    auto cost = [&](int i) {
+        return (double)params[i].n * (double)params[i].maxiter * (double)std::max<bbjd_int>(params[i].maxsub, 1);
+    };
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost(a) > cost(b); });
     std::atomic<int> next{0};
     std::vector<bbjd_status> st(count, BBJD_SUCCESS);
+    const int nt = std::min(threads, std::max(count, 1));
     auto worker = [&]() {
         cudaSetDevice(dev);
+        g_concurrent_solve = true;
         for (;;) {
-            const int i = next.fetch_add(1);
-            if (i >= count) break;
+            const int q = next.fetch_add(1);
+            if (q >= count) break;
+            const int i = order[q];
             bbjd_device_ext local;
             bbjd_device_ext_init(&local);
             bbjd_device_ext *e = exts ? &exts[i] : &local;
             st[i] = bbjd_solve_device(&params[i], e, mats[i], pcs[i], wss[i], &results[i]);
         }
     };
-    const int nt = std::min(threads, std::max(count, 1));
     std::vector<std::thread> pool;
     for (int t = 0; t < nt; ++t) pool.emplace_back(worker);
     for (auto &th : pool) th.join();

@@ -30,6 +30,12 @@ Operators *make_device_ops(const bbjd_bbt_matrix *m, const bbjd_precond *pc, Scr
                            cudaStream_t st);
 Operators *make_callback_ops(const bbjd_params *p, Scratch *S, cudaStream_t st, int *cb_failed);
 
+// Set on the host threads of bbjd_solve_batch: their projected solves take
+// the OpenBLAS path (with a solve on every core, MKL's ZGEEV was measured
+// slower than OpenBLAS on the B200 host; alone it is faster), whatever the
+// thread count, so a batch returns the same bits with 1 or N threads.
+extern thread_local bool g_concurrent_solve;
+
 enum KClass { KC_SPMV = 0, KC_ORTH, KC_PENCIL, KC_RITZ, KC_PRECOND, KC_RESTART, KC_SMALL, KC_GMRES, KC_N };
 
 // Device timing of kernel classes with CUDA events on the solve's stream.

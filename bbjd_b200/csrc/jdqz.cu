@@ -55,6 +55,10 @@ void scipy_ztrsen_(const char *job, const char *compq, const int *select, const 
 // 27.2 ms, one thread).  It is looked up once per process, by the path the
 // build recorded, and called with one MKL thread (thread-local setting,
 // restored afterwards).  Without it the OpenBLAS path runs.
+namespace bbjd {
+thread_local bool g_concurrent_solve = false;
+}
+
 namespace {
 typedef void (*zgeev_fn)(const char *, const char *, const int *, bbjd_zomplex *, const int *,
                          bbjd_zomplex *, bbjd_zomplex *, const int *, bbjd_zomplex *, const int *,
@@ -500,7 +504,7 @@ int Engine::solve_projected_schur(int k, int nkeep, bool reorder, int *target_po
     };
     const int lw = (int)zwork.size();
     const MklLapack &mkl = mkl_lapack();
-    if (!reorder && mkl.zgeev) {
+    if (!reorder && mkl.zgeev && !g_concurrent_solve) {
         // Between restarts only the eigenvalues and the target's eigenvector
         // are used: eigenvalues by ZGEEV on a copy of H (no vectors), the
         // target's eigenvector by inverse iteration with a dense LU of

@@ -140,7 +140,8 @@ bbjd_status bbjd_solve_device(const bbjd_params *params, bbjd_device_ext *ext,
  * uses params[i], mats[i], pcs[i] (may be NULL), wss[i], results[i] and, when
  * exts != NULL, exts[i].  Up to `threads` solves run at once, each on its own
  * host thread and CUDA stream, so the host-side projected QZ of one solve
- * overlaps the device work of the others.  Every params[i].v0 must be set
+ * overlaps the device work of the others; solves start largest first (by
+ * n x maxiter x maxsub).  Every params[i].v0 must be set
  * (the seeded start vector uses the C library's global rand()), and no two
  * solves may share a matrix or preconditioner handle (their scratch is not
  * shared-safe).  Returns the first failing status, else BBJD_SUCCESS (or
