@@ -178,3 +178,27 @@ def test_jdqz_device_reports_error_vs_oracle():
     assert info["nconv"] == int(g["k"])
     assert info["error_vs_oracle"] == pytest.approx(match_set(ev, g["eigenvalues"]).max())
     assert info["error_vs_oracle"] < EIG_ATOL
+
+
+def test_device_maxiter_returns_partial_result():
+    """Stopping at maxiter is not an error (status 1, reference bbjd.py:262-266):
+    the pairs found so far come back, with a RuntimeWarning at verbose >= 1."""
+    P = make_pencil(16, 64, 8, seed=0)
+    with pytest.warns(RuntimeWarning):
+        ev, evecs, info = jdqz(P, k=6, sigma=3.0, maxiter=12, maxsub=20, minsub=8,
+                               preconditioner="exact", v0=start_vector(P.n, 1),
+                               return_info=True, verbose=1)
+    assert info["status"] == 1 and info["nconv"] < 6
+    assert ev.shape == (info["nconv"],) and evecs.shape == (P.n, info["nconv"])
+    assert len(info["residuals"]) == info["nconv"]
+
+
+@pytest.mark.parametrize("bad", [dict(k=0), dict(tol=-1.0), dict(k=10_000)])
+def test_device_invalid_parameters_raise(bad):
+    P = make_pencil(8, 16, 2, seed=0)
+    kw = dict(k=2, sigma=3.0, tol=1e-10, preconditioner="exact", v0=start_vector(P.n, 1))
+    kw.update(bad)
+    # as the reference: a parameter the C core rejects is a RuntimeError, a
+    # workspace it cannot allocate a MemoryError (reference _bbjd_c.c:199-200)
+    with pytest.raises((RuntimeError, ValueError, MemoryError)):
+        jdqz(P, **kw)
