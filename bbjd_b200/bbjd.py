@@ -532,15 +532,28 @@ def jdqz_batch(pencils, sigmas, k: int = 6, tol: float = 1e-10, maxiter: int = 2
     """Independent 'nearest sigma' solves of a sigma-sweep on one GPU
     (bbjd_solve_batch): solve i is ``jdqz(pencils[i], k=k, sigma=sigmas[i],
     ...)``; up to `threads` run at once, each on its own host thread and
-    CUDA stream.  Returns a list of ``(eigenvalues, eigenvectors, info)``
-    and the batch's wall time in seconds.  Results equal those of the same
-    solves run one at a time."""
+    CUDA stream, largest pencils first.  Solves may share a pencil (it is
+    uploaded once).  Returns a list of ``(eigenvalues, eigenvectors, info)``
+    and the batch's wall time in seconds.  The results do not depend on
+    `threads` (the batch's projected eigenvalues always come from OpenBLAS,
+    so they can differ from a single ``jdqz`` call, which may use MKL, by
+    rounding)."""
     import time as _time
     lib = _lib.load()
     count = len(pencils)
     if len(sigmas) != count:
         raise ValueError("one sigma per pencil")
-    devs = [p if isinstance(p, DevicePencil) else DevicePencil(p) for p in pencils]
+    # one device copy per distinct pencil: the solves of a sweep over sigma
+    # of the same pencil share it (read-only during the solves)
+    uploaded: dict = {}
+    devs = []
+    for p in pencils:
+        if isinstance(p, DevicePencil):
+            devs.append(p)
+        else:
+            if id(p) not in uploaded:
+                uploaded[id(p)] = DevicePencil(p)
+            devs.append(uploaded[id(p)])
     pcs = [DevicePreconditioner(d, s, preconditioner, precision=precision) if preconditioner
            else None for d, s in zip(devs, sigmas)]
     if v0s is None:

@@ -369,8 +369,7 @@ bbjd_status bbjd_solve_batch(int count, const bbjd_params *params, bbjd_device_e
     for (int i = 0; i < count; ++i) {
         if (!params[i].v0 || !mats[i] || !wss[i]) return BBJD_ERR_INVALID;
         for (int j = 0; j < i; ++j)
-            if (mats[j] == mats[i] || (pcs[i] && pcs[j] == pcs[i]) || wss[j] == wss[i])
-                return BBJD_ERR_INVALID;
+            if ((pcs[i] && pcs[j] == pcs[i]) || wss[j] == wss[i]) return BBJD_ERR_INVALID;
     }
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return BBJD_ERR_CUDA;

@@ -143,8 +143,9 @@ bbjd_status bbjd_solve_device(const bbjd_params *params, bbjd_device_ext *ext,
  * overlaps the device work of the others; solves start largest first (by
  * n x maxiter x maxsub).  Every params[i].v0 must be set
  * (the seeded start vector uses the C library's global rand()), and no two
- * solves may share a matrix or preconditioner handle (their scratch is not
- * shared-safe).  Returns the first failing status, else BBJD_SUCCESS (or
+ * solves may share a preconditioner or a workspace (their scratch is
+ * written during the solve); solves may share a matrix (a sweep over sigma
+ * of one pencil: each solve reads it and has its own product scratch).  Returns the first failing status, else BBJD_SUCCESS (or
  * BBJD_MAX_ITER if any solve stopped at maxiter). */
 bbjd_status bbjd_solve_batch(int count, const bbjd_params *params, bbjd_device_ext *exts,
                              const bbjd_bbt_matrix *const *mats, const bbjd_precond *const *pcs,
