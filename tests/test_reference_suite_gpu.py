@@ -229,3 +229,71 @@ def test_jdqz_c_tuple_contract():
                                                   lu.solve, tol=1e-10)
     assert nconv == 2 and status == 0 and evecs.shape == (12, 2) and res.shape == (2,)
     assert np.all(res < 1e-10) and iters >= 1
+
+
+def _golden_random():
+    g = dict(np.load(os.path.join(GOLDEN, "random200.npz")))
+    n = int(g["n"])
+    A = sp.csr_matrix((g["A_data"], g["A_indices"], g["A_indptr"]), shape=(n, n))
+    return g, A, sp.eye(n, format="csr", dtype=np.complex128)
+
+
+def test_random_fewer_eigenvalues():               # reference :263-279
+    from scipy.sparse.linalg import eigs
+    g, A, B = _golden_random()
+    sigma = complex(g["sigma"])
+    ref, _ = eigs(A, k=3, sigma=sigma, which="LM")
+    ev, _, info = jdqz(A, B, k=3, sigma=sigma, tol=1e-10, preconditioner=LU(A - sigma * B),
+                       return_info=True, maxiter=500)
+    assert info["nconv"] == 3
+    assert match_set(ev, ref).max() < 1e-8
+
+
+def test_target_found_after_locking():             # reference :556-578
+    # after the first lock the target is scanned for over all positions,
+    # not read from position `locked`: all three pairs converge
+    g, A, B = _golden_random()
+    sigma = complex(g["sigma"])
+    _, _, info = jdqz(A, B, k=3, sigma=sigma, tol=1e-10, preconditioner=LU(A - sigma * B),
+                      return_info=True, maxiter=500, maxsub=150, minsub=60)
+    assert info["nconv"] == 3
+
+
+def _banded_with_tau(n, bandwidth=7, n_tau=4, shift=3.0, seed=123):
+    """Banded random matrix with dense leading rows (spectral-PDE shape, the
+    reference suite's block-banded + tau case), B = I."""
+    rng = np.random.default_rng(seed)
+    offsets = list(range(-bandwidth, bandwidth + 1))
+    diags = [rng.standard_normal(n - abs(o)) + 0.1j * rng.standard_normal(n - abs(o)) for o in offsets]
+    A = sp.diags(diags, offsets, shape=(n, n), format="lil", dtype=np.complex128)
+    for i in range(n_tau):
+        A[i, :] = rng.standard_normal(n) + 0.1j * rng.standard_normal(n)
+    A = A.tocsr() + shift * sp.eye(n, dtype=np.complex128)
+    return A, sp.eye(n, format="csr", dtype=np.complex128)
+
+
+def test_block_banded_tau():                       # reference :290-318
+    import scipy.linalg as sl
+    A, B = _banded_with_tau(300)
+    sigma = 3.0 + 0j
+    lam = sl.eigvals(A.toarray())
+    ref = lam[np.argsort(np.abs(lam - sigma))[:6]]
+    ev, evecs, info = jdqz(A, B, k=6, sigma=sigma, tol=1e-10, preconditioner=LU(A - sigma * B),
+                           return_info=True, maxiter=500, maxsub=150, minsub=60)
+    assert info["nconv"] == 6
+    assert match_set(ev, ref).max() < 1e-8
+    for j in range(6):
+        assert residual(A, B, ev[j], evecs[:, j]) < 1e-8
+
+
+def test_larger_random():                          # reference :631-647
+    n = 500
+    rng = np.random.default_rng(42)
+    A = sp.random(n, n, density=0.02, format="csr", dtype=np.complex128, random_state=7)
+    A = A + 5 * sp.eye(n, dtype=np.complex128)
+    A.data += 0.1j * rng.standard_normal(A.nnz)
+    B = sp.eye(n, format="csr", dtype=np.complex128)
+    sigma = 5.0 + 0j
+    _, _, info = jdqz(A, B, k=5, sigma=sigma, tol=1e-10, preconditioner=LU(A - sigma * B),
+                      return_info=True, maxiter=500, maxsub=100, minsub=40)
+    assert info["nconv"] >= 3
