@@ -202,3 +202,21 @@ def test_device_invalid_parameters_raise(bad):
     # workspace it cannot allocate a MemoryError (reference _bbjd_c.c:199-200)
     with pytest.raises((RuntimeError, ValueError, MemoryError)):
         jdqz(P, **kw)
+
+
+def test_full_size_pairs_satisfy_host_residual():
+    """The benchmark's n = 1,000,064 pencil (b = 32, 31,250 blocks, t = 64),
+    150 outer iterations: every returned pair satisfies the normalised
+    residual test computed on the host with the numpy block product (a
+    check independent of the device kernels), and no value repeats."""
+    P = make_pencil(32, 31250, 64, seed=0)
+    ev, evecs, info = jdqz(P, k=64, sigma=3.0, tol=1e-10, maxiter=150, maxsub=200, minsub=80,
+                           preconditioner="exact", v0=start_vector(P.n, 1), return_info=True)
+    assert info["nconv"] >= 1
+    nA = np.sqrt(sum(np.vdot(a, a).real for a in (P.Ad, P.Al, P.Au, P.E, P.F)))
+    nB = np.sqrt(np.vdot(P.Bd, P.Bd).real)
+    for lam, x in zip(ev, evecs.T):
+        r = P.matvec_A(x) - lam * P.matvec_B(x)
+        assert np.linalg.norm(r) / ((nA + abs(lam) * nB) * np.linalg.norm(x)) < 1e-10
+    assert np.all(info["residuals"] < 1e-10)
+    assert_no_duplicates(ev)
