@@ -4,6 +4,8 @@
                                 [--iters 30] [--maxsub 200] [--minsub 80]
                                 [--preconditioner exact|block_jacobi]
                                 [--inner-maxiter 0] [--inner-tol 1e-2]
+                                [--projected auto|qz|schur] [--lock robust|reference]
+                                [--precision fp64|mixed] [--verbose 0|1|2]
     python -m bbjd_b200.profile --sweep 32 [--threads 16] [--maxiter 2000]
 
 Builds the seeded pencil, uploads it, factors the exact LU (or the block
@@ -63,6 +65,7 @@ def main(argv=None):
     ap.add_argument("--inner-maxiter", type=int, default=0)
     ap.add_argument("--inner-tol", type=float, default=1e-2)
     ap.add_argument("--verbose", type=int, default=0)
+    ap.add_argument("--lock", default="robust", choices=["robust", "reference"])
     a = ap.parse_args(argv)
     if a.sweep:
         return sweep(a.sweep, a.threads, a.precision, a.maxiter)
@@ -73,7 +76,7 @@ def main(argv=None):
     ev, _, info = jdqz(dev, k=a.k, sigma=3.0, tol=1e-10, maxiter=a.iters, maxsub=a.maxsub,
                        minsub=a.minsub, inner_maxiter=a.inner_maxiter, inner_tol=a.inner_tol,
                        preconditioner=pc, v0=start_vector(P.n, 1), verbose=a.verbose,
-                       return_info=True, timing=True, projected=a.projected,
+                       return_info=True, timing=True, projected=a.projected, lock=a.lock,
                        precision=a.precision)
     wall = time.time() - t0
     d = info["device"]
