@@ -77,7 +77,8 @@ def test_rejects_other_structures():
     A[0, 3 * 8 + 1] = rng.standard_normal()
     assert structure.detect(A.tocsr(), P.to_csc("B")) == (16, 3)
     # a block-tridiagonal matrix with 24 x 24 blocks fits none of 8, 16, 32
-    blocks = sp.kron(sp.diags([1, 1, 1], [-1, 0, 1], shape=(8, 8)), np.ones((24, 24)))
+    blocks = sp.kron(sp.diags([1.0, 1.0, 1.0], [-1, 0, 1], shape=(8, 8), dtype=np.float64),
+                     np.ones((24, 24)))
     assert structure.detect(blocks.tocsr(), None, b_is_identity=True) is None
 
 
