@@ -54,6 +54,24 @@ class DevicePencil:
             b, nblk, t = pencil.b, pencil.nblk, pencil.t
         elif arrays is None:
             raise ValueError("pass a BBTPencil or its device-layout arrays")
+        else:
+            nb, n = b * nblk, b * nblk + t
+            want = {"Ad": nblk * b * b, "Al": nblk * b * b, "Au": nblk * b * b,
+                    "Bd": nblk * b * b, "E": nb * t, "FT": n * t}
+            for name, count in want.items():
+                if name not in arrays:
+                    if count:
+                        raise ValueError(f"arrays lacks {name!r}")
+                    continue
+                a = arrays[name]
+                if hasattr(a, "data_ptr"):
+                    nbytes, contiguous = a.numel() * a.element_size(), a.is_contiguous()
+                else:
+                    nbytes, contiguous = a.nbytes, a.flags.c_contiguous or a.flags.f_contiguous
+                if nbytes != 16 * count or not contiguous:
+                    raise ValueError(f"{name!r} must be {count} contiguous complex128 values "
+                                     f"({16 * count} bytes); got {nbytes} bytes"
+                                     + ("" if contiguous else ", not contiguous"))
         addr = lambda a: a.data_ptr() if hasattr(a, "data_ptr") else _lib.ptr(a)  # noqa: E731
         h = C.c_void_p()
         st = lib.bbjd_bbt_create(b, nblk, t, addr(arrays["Ad"]), addr(arrays["Al"]),

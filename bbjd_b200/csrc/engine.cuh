@@ -103,6 +103,10 @@ struct Engine {
     bool schur_step = false;          // the last projected solve used the Schur form
     bool ritz_ready = false;          // hx holds the target's coefficients already
     std::vector<zc> hC, hT, hx, tau, omega;
+    // H of the last Schur-form projected solve (k = hH_k, ld maxsub; 0 = none)
+    // and the iterations since it was last formed in full
+    std::vector<zc> hH, hxs, hys;
+    int hH_k = 0, hH_age = 0;
     std::vector<int> ipiv;
     double qz_seconds = 0;
     // host seconds of the Schur-form projected solve: forming H, Hessenberg

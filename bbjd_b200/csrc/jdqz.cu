@@ -206,6 +206,11 @@ bbjd_status Engine::init(const bbjd_params *p, bbjd_workspace *w, bbjd_result *r
     sel.resize(maxsub);
     hC.resize((size_t)maxsub * maxsub);
     hT.resize((size_t)maxsub * maxsub);
+    hH.resize((size_t)maxsub * maxsub);
+    hxs.resize(maxsub);
+    hys.resize(maxsub);
+    hH_k = 0;
+    hH_age = 0;
     hx.resize(maxsub);
     tau.resize(maxsub);
     omega.resize(maxsub);
@@ -374,6 +379,7 @@ static double target_value(zc lam, zc sigma, int target) {
 int Engine::solve_projected(int k, int locked, int nkeep, int *target_pos) {
     (void)locked;
     ritz_ready = false;
+    hH_k = 0;
     auto t0 = std::chrono::steady_clock::now();
     const int bk = k, lda = (int)maxsub;
     zc *MA = ws->MA, *MB = ws->MB, *SA = ws->SA, *SB = ws->SB, *ZA = ws->ZA, *ZB = ws->ZB;
@@ -483,17 +489,61 @@ int Engine::solve_projected_schur(int k, int nkeep, bool reorder, int *target_po
     // columns and the locked Q_left), so C = W^H (nu0 A + mu0 B) V is upper
     // triangular up to rounding and one triangular solve gives H.  Should the
     // part below the diagonal exceed 1e-14 of ||C||_F, LU with pivoting.
-    if (c_low <= 1e-28 * c_all) {
+    const bool tri = c_low <= 1e-28 * c_all;
+    if (tri && hH_k == k - 1 && k > 1 && hH_age < 32) {
+        // One column and row more than the last H (nothing else changed):
+        // with C = [[C0, c], [0, g]] and MB = [[MB0, b], [m^T, beta]],
+        //   H = [[H0 - x m^T, C0^-1 b - x beta], [m^T / g, beta / g]],
+        // x = C0^-1 c / g: two triangular solves and a rank-one update,
+        // O(k^2) instead of the O(k^3) solve.  Rebuilt in full every 32
+        // iterations so rounding cannot accumulate.
+        const int k0 = k - 1;
+        const size_t L = maxsub;
+        const zc g = hC[k0 + (size_t)k0 * L];
+        if (std::abs(g) == 0.0) return 1;
+        std::vector<zc> &x = hxs, &y = hys;
+        for (int i = 0; i < k0; ++i) {
+            x[i] = hC[i + (size_t)k0 * L];
+            y[i] = MB[i + (size_t)k0 * L];
+        }
+        for (int i = k0 - 1; i >= 0; --i) {            // C0 x = c, C0 y = b (upper)
+            zc ax = x[i], ay = y[i];
+            for (int j = i + 1; j < k0; ++j) {
+                ax -= hC[i + (size_t)j * L] * x[j];
+                ay -= hC[i + (size_t)j * L] * y[j];
+            }
+            const zc d = hC[i + (size_t)i * L];
+            if (std::abs(d) == 0.0) return 1;
+            x[i] = ax / d;
+            y[i] = ay / d;
+        }
+        const zc beta_ = MB[k0 + (size_t)k0 * L];
+        for (int i = 0; i < k0; ++i) x[i] /= g;
+        for (int j = 0; j < k0; ++j) {
+            const zc mj = MB[k0 + (size_t)j * L];
+            for (int i = 0; i < k0; ++i) T[i + (size_t)j * L] = hH[i + (size_t)j * L] - x[i] * mj;
+            T[k0 + (size_t)j * L] = mj / g;
+        }
+        for (int i = 0; i < k0; ++i) T[i + (size_t)k0 * L] = y[i] - x[i] * beta_;
+        T[k0 + (size_t)k0 * L] = beta_ / g;
+        hH_age++;
+    } else if (tri) {
         scipy_ztrtrs_("U", "N", "N", &bk, &bk, hC.data(), &ld, T, &ld, &info);
         if (info > 0) return 1;
         if (info < 0) return -1;
+        hH_age = 0;
     } else {
         scipy_zgetrf_(&bk, &bk, hC.data(), &ld, ipiv.data(), &info);
         if (info > 0) return 1;
         if (info < 0) return -1;
         scipy_zgetrs_("N", &bk, &bk, hC.data(), &ld, ipiv.data(), T, &ld, &info);
         if (info) return -1;
+        hH_age = 0;
     }
+    // H as it is now (T itself is overwritten by the Hessenberg reduction or
+    // the Schur form below): the base of the next iteration's update
+    for (int j = 0; j < k; ++j) memcpy(&hH[(size_t)j * maxsub], T + (size_t)j * maxsub, sizeof(zc) * k);
+    hH_k = k;
     auto t1 = std::chrono::steady_clock::now();
     qz_split[0] += std::chrono::duration<double>(t1 - t0).count();
     auto to_lambda = [&](int i) {
@@ -1117,6 +1167,7 @@ bbjd_status Engine::run() {
             }
             ws->kdim = keep;
             k = keep;
+            hH_k = 0;                    // MA, MB were rebuilt: H starts over
         }
         // expansion (jd_core.c:1033-1048)
         cplx *vnew = V + k * ld;

@@ -140,12 +140,16 @@ class BBTPencil:
         of 32 rows with one coalesced 512-byte transaction; ``E`` is
         column-major (ld = nb); ``F`` is stored transposed, ``FT[col][tau]``,
         so that a warp reads the t tau entries of one column contiguously.
+        Every array is returned flat (1-D, contiguous) in that order, so a
+        caller that copies or reinterprets it (pinned buffers, ``.view``)
+        cannot reorder it by accident.
         """
-        tr = lambda a: np.ascontiguousarray(np.transpose(a, (0, 2, 1)))  # noqa: E731
+        tr = lambda a: np.ascontiguousarray(np.transpose(a, (0, 2, 1))).reshape(-1)  # noqa: E731
+        none = np.zeros((0,), np.complex128)
         return {
             "Ad": tr(self.Ad), "Al": tr(self.Al), "Au": tr(self.Au), "Bd": tr(self.Bd),
-            "E": np.asfortranarray(self.E) if self.t else np.zeros((0,), np.complex128),
-            "FT": np.ascontiguousarray(self.F.T) if self.t else np.zeros((0,), np.complex128),
+            "E": np.ascontiguousarray(self.E.T).reshape(-1) if self.t else none,
+            "FT": np.ascontiguousarray(self.F.T).reshape(-1) if self.t else none,
         }
 
 

@@ -104,6 +104,22 @@ def test_device_v0_length_checked():
         jdqz(P, k=1, sigma=3.0, preconditioner="exact", v0=np.ones(P.n - 1))
 
 
+def test_pinned_arrays_are_the_same_pencil():
+    """A pencil uploaded from pinned torch copies of its device arrays (the
+    end-to-end input path) is the pencil uploaded from the BBTPencil: the
+    same solve gives bitwise the same eigenvalues."""
+    import torch
+    P = make_pencil(16, 40, 8, seed=2)
+    pinned = {k: torch.from_numpy(v.view(np.float64)).pin_memory()
+              for k, v in P.device_arrays().items()}
+    kw = dict(k=3, sigma=3.0, preconditioner="exact", maxsub=24, minsub=10, maxiter=300,
+              v0=start_vector(P.n, 1))
+    ev_a = jdqz(P, **kw)[0]
+    ev_b = jdqz(DevicePencil(arrays=pinned, b=16, nblk=40, t=8), **kw)[0]
+    assert len(ev_a) == 3
+    np.testing.assert_array_equal(ev_a, ev_b)
+
+
 def test_device_stats_reported():
     P = make_pencil(16, 64, 8, seed=0)
     ev, evecs, info = jdqz(P, k=2, sigma=3.0, preconditioner="exact", maxsub=20, minsub=8,

@@ -42,8 +42,12 @@ def test_device_layout_is_column_major():
     d = P.device_arrays()
     j, i, c = 2, 3, 5
     assert d["Ad"].reshape(-1)[j * 64 + c * 8 + i] == P.Ad[j, i, c]
-    assert d["E"].reshape(-1, order="F")[1 * P.nb + 7] == P.E[7, 1]
-    assert d["FT"].reshape(-1)[9 * 2 + 1] == P.F[1, 9]
+    assert d["E"][1 * P.nb + 7] == P.E[7, 1]
+    assert d["FT"][9 * 2 + 1] == P.F[1, 9]
+    # flat and contiguous: a reshape or a float64 view keeps the order
+    for name, a in d.items():
+        assert a.ndim == 1 and a.flags.c_contiguous, name
+        np.testing.assert_array_equal(a.reshape(-1).view(np.float64).view(np.complex128), a)
 
 
 def test_shifted_pencil():
