@@ -303,11 +303,12 @@ def jdqz_c(n, nev, sigma, target, matvec_A, matvec_B, precond_solve, tol=1e-10, 
 
 _PROJECTED = {"auto": 0, "qz": 1, "schur": 2}
 _LOCK = {"robust": 0, "reference": 1}
+_RITZ = {"auto": 0, "fp64": 1, "fp32": 2}
 
 
 def _solve_device(dev: DevicePencil, pc, k, sigma, target, tol, maxiter, maxsub, minsub,
                   inner_maxiter, inner_tol, v0, verbose, timing, projected="auto",
-                  lock="robust", precision="fp64"):
+                  lock="robust", precision="fp64", ritz_estimate="auto"):
     lib = _lib.load()
     n = dev.n
     p = _lib.Params()
@@ -332,6 +333,9 @@ def _solve_device(dev: DevicePencil, pc, k, sigma, target, tol, maxiter, maxsub,
     if lock not in _LOCK:
         raise ValueError(f"lock must be one of {list(_LOCK)}")
     ext.lock_rule = _LOCK[lock]
+    if ritz_estimate not in _RITZ:
+        raise ValueError(f"ritz_estimate must be one of {list(_RITZ)}")
+    ext.ritz_estimate = _RITZ[ritz_estimate]
     ext.evec_layout = 1        # BBJD_EVEC_ROW_MAJOR: the (n, nconv) array comes back ready
     ws = lib.bbjd_workspace_alloc(C.byref(p))
     if not ws:
@@ -351,7 +355,8 @@ def _solve_device(dev: DevicePencil, pc, k, sigma, target, tol, maxiter, maxsub,
         "seconds_device": ext.seconds_device, "seconds_restart": ext.seconds_restart,
         "bytes_device": ext.bytes_device, "kernel_launches": int(ext.kernel_launches),
         "dgks_passes": int(ext.dgks_passes), "restarts": int(ext.restarts),
-        "duplicates": int(ext.duplicates),
+        "duplicates": int(ext.duplicates), "ritz_refinements": int(ext.ritz_refinements),
+        "ritz_fallbacks": int(ext.ritz_fallbacks),
         "kernels": {name: {"ms": ext.kernel_ms[i], "bytes": ext.kernel_bytes[i],
                            "calls": int(ext.kernel_calls[i])}
                     for i, name in enumerate(_lib.KERNEL_CLASSES)},
@@ -380,6 +385,7 @@ def jdqz(
     lock: str = "robust",
     precision: str = "fp64",
     oracle=None,
+    ritz_estimate: str = "auto",
 ):
     """Jacobi-Davidson QZ for ``A x = lambda B x``, the eigenvalues nearest
     ``sigma`` first.  Parameters, defaults, returns and errors are those of
@@ -406,7 +412,12 @@ def jdqz(
     and QZ stay FP64).  ``oracle``: reference eigenvalues (e.g. from an FP64
     run or ARPACK); with ``return_info`` the info dict then holds
     ``error_vs_oracle``, the largest distance from a returned eigenvalue to
-    its nearest oracle value.
+    its nearest oracle value.  ``ritz_estimate`` (Schur form only): 'fp32'
+    ('auto') ranks the candidates between restarts by complex64 estimates
+    of the projected eigenvalues and refines the chosen one to an FP64
+    eigenpair by Rayleigh-quotient iteration (the FP64 path takes over when
+    that does not converge); 'fp64' computes all of them in FP64.  The
+    returned values and the convergence test are FP64 either way.
     """
     if which not in _TARGET_MAP:
         raise ValueError(f"which must be one of {list(_TARGET_MAP.keys())}; got {which!r}")
@@ -436,7 +447,7 @@ def jdqz(
         try:
             ev, evecs, resid, nconv, iters, status, stats = _solve_device(
                 dev, pc, k, sigma, target, tol, maxiter, maxsub, minsub, inner_maxiter,
-                inner_tol, v0, verbose, timing, projected, lock, precision)
+                inner_tol, v0, verbose, timing, projected, lock, precision, ritz_estimate)
         finally:
             if own_pc:
                 pc.close()
@@ -461,7 +472,8 @@ def jdqz(
                         maxsub=maxsub, minsub=minsub, inner_maxiter=inner_maxiter,
                         inner_tol=inner_tol, preconditioner=pc, v0=v0, verbose=verbose,
                         return_info=return_info, timing=timing, projected=projected,
-                        lock=lock, precision=precision, oracle=oracle)
+                        lock=lock, precision=precision, oracle=oracle,
+                        ritz_estimate=ritz_estimate)
         if isinstance(preconditioner, (str, SparseLU, DevicePreconditioner)):
             raise ValueError("a device preconditioner needs a block-bordered A, B pencil")
 
@@ -546,7 +558,7 @@ def jdqz_device(pencil, **kwargs):
 def jdqz_batch(pencils, sigmas, k: int = 6, tol: float = 1e-10, maxiter: int = 200,
                maxsub: int = 0, minsub: int = 0, preconditioner: str = "exact",
                precision: str = "fp64", v0s=None, threads: int = 8, projected: str = "auto",
-               lock: str = "robust"):
+               lock: str = "robust", ritz_estimate: str = "auto"):
     """Independent 'nearest sigma' solves of a sigma-sweep on one GPU
     (bbjd_solve_batch): solve i is ``jdqz(pencils[i], k=k, sigma=sigmas[i],
     ...)``; up to `threads` run at once, each on its own host thread and
@@ -561,6 +573,8 @@ def jdqz_batch(pencils, sigmas, k: int = 6, tol: float = 1e-10, maxiter: int = 2
     count = len(pencils)
     if len(sigmas) != count:
         raise ValueError("one sigma per pencil")
+    if ritz_estimate not in _RITZ:
+        raise ValueError(f"ritz_estimate must be one of {list(_RITZ)}")
     # one device copy per distinct pencil: the solves of a sweep over sigma
     # of the same pencil share it (read-only during the solves)
     uploaded: dict = {}
@@ -597,6 +611,7 @@ def jdqz_batch(pencils, sigmas, k: int = 6, tol: float = 1e-10, maxiter: int = 2
         exts[i].precision = 1 if precision == "mixed" else 0
         exts[i].projected = _PROJECTED[projected]
         exts[i].lock_rule = _LOCK[lock]
+        exts[i].ritz_estimate = _RITZ[ritz_estimate]
         exts[i].evec_layout = 1
         wss[i] = lib.bbjd_workspace_alloc(C.byref(p))
         if not wss[i]:

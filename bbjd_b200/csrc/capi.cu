@@ -168,8 +168,9 @@ static bbjd_status run_engine(const bbjd_params *p, bbjd_workspace *ws, bbjd_res
     if (s == BBJD_SUCCESS) s = E.run();
     if (p->verbose >= 1 && E.proj_mode == BBJD_PROJ_SCHUR)
         fprintf(stderr, "  projected solve %.3f s: form H %.3f, Hessenberg %.3f, eigenvalues %.3f, "
-                "target vector %.3f, restart Schur form + reorder %.3f\n", E.qz_seconds, E.qz_split[0],
-                E.qz_split[1], E.qz_split[2], E.qz_split[3], E.qz_split[4]);
+                "target vector %.3f, restart Schur form + reorder %.3f (FP32 estimates: %lld "
+                "refinement LUs, %lld FP64 fallbacks)\n", E.qz_seconds, E.qz_split[0],
+                E.qz_split[1], E.qz_split[2], E.qz_split[3], E.qz_split[4], E.rq_lus, E.rq_fallbacks);
     if (s != BBJD_ERR_CUDA && !(cb_failed && *cb_failed)) {
         const bbjd_status f = E.finish_eigenvectors();
         if (f != BBJD_SUCCESS) s = f;
@@ -187,6 +188,8 @@ static bbjd_status run_engine(const bbjd_params *p, bbjd_workspace *ws, bbjd_res
         ext->dgks_passes = E.dgks;
         ext->restarts = E.restarts;
         ext->duplicates = E.duplicates;
+        ext->ritz_refinements = E.rq_lus;
+        ext->ritz_fallbacks = E.rq_fallbacks;
         double dev = 0.0;
         E.T.flush();
         for (int c = 0; c < KC_N && c < 8; ++c) {

@@ -107,6 +107,12 @@ struct Engine {
     // and the iterations since it was last formed in full
     std::vector<zc> hH, hxs, hys;
     int hH_k = 0, hH_age = 0;
+    // complex64 copy of H and LAPACK workspace for the FP32 eigenvalue
+    // estimates (BBJD_RITZ_FP32); refinement LU count and FP64 fallbacks
+    bool ritz32 = true;
+    std::vector<std::complex<float>> hC32, w32, zwork32, tau32;
+    std::vector<float> rwork32;
+    long long rq_lus = 0, rq_fallbacks = 0;
     std::vector<int> ipiv;
     double qz_seconds = 0;
     // host seconds of the Schur-form projected solve: forming H, Hessenberg
@@ -141,6 +147,10 @@ struct Engine {
     int solve_projected_schur(int k, int nkeep, bool reorder, int *target_pos);
     void hessenberg_eigvec(int k, zc w, zc *x);
     void dense_eigvec(int k, zc w, zc *x);
+    bool eigenvalues32(int k);
+    bool rq_refine(int k, zc &w, zc *x);
+    bool refine_target(int k, int *target_pos);
+    void to_lambda(int i);
     void select_and_scan(int k, int nkeep, int *target_pos);
     void ritz_coefficients(int k, int p, zc ta, zc tb, cplx *x);
     bbjd_status sync();

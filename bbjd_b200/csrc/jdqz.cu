@@ -42,6 +42,13 @@ void scipy_zunghr_(const int *n, const int *ilo, const int *ihi, bbjd_zomplex *a
 void scipy_zhseqr_(const char *job, const char *compz, const int *n, const int *ilo, const int *ihi,
                    bbjd_zomplex *h, const int *ldh, bbjd_zomplex *w, bbjd_zomplex *z, const int *ldz,
                    bbjd_zomplex *work, const int *lwork, int *info);
+void scipy_cgehrd_(const int *n, const int *ilo, const int *ihi, std::complex<float> *a,
+                   const int *lda, std::complex<float> *tau, std::complex<float> *work,
+                   const int *lwork, int *info);
+void scipy_chseqr_(const char *job, const char *compz, const int *n, const int *ilo, const int *ihi,
+                   std::complex<float> *h, const int *ldh, std::complex<float> *w,
+                   std::complex<float> *z, const int *ldz, std::complex<float> *work,
+                   const int *lwork, int *info);
 void scipy_ztrsen_(const char *job, const char *compq, const int *select, const int *n,
                    bbjd_zomplex *t, const int *ldt, bbjd_zomplex *q, const int *ldq, bbjd_zomplex *w,
                    int *m, double *s, double *sep, bbjd_zomplex *work, const int *lwork, int *info);
@@ -63,9 +70,14 @@ namespace {
 typedef void (*zgeev_fn)(const char *, const char *, const int *, bbjd_zomplex *, const int *,
                          bbjd_zomplex *, bbjd_zomplex *, const int *, bbjd_zomplex *, const int *,
                          bbjd_zomplex *, const int *, double *, int *);
+typedef void (*cgeev_fn)(const char *, const char *, const int *, std::complex<float> *, const int *,
+                         std::complex<float> *, std::complex<float> *, const int *,
+                         std::complex<float> *, const int *, std::complex<float> *, const int *,
+                         float *, int *);
 typedef int (*mkl_threads_fn)(int);
 struct MklLapack {
     zgeev_fn zgeev = nullptr;
+    cgeev_fn cgeev = nullptr;
     mkl_threads_fn set_local_threads = nullptr;
 };
 const MklLapack &mkl_lapack() {
@@ -80,6 +92,7 @@ const MklLapack &mkl_lapack() {
         auto t = (mkl_threads_fn)dlsym(h, "MKL_Set_Num_Threads_Local");
         if (g && t) {
             m.zgeev = g;
+            m.cgeev = (cgeev_fn)dlsym(h, "cgeev_");
             m.set_local_threads = t;
         }
 #endif
@@ -216,6 +229,15 @@ bbjd_status Engine::init(const bbjd_params *p, bbjd_workspace *w, bbjd_result *r
     omega.resize(maxsub);
     ipiv.resize(maxsub);
     zwork.resize(64 * (size_t)maxsub + 64);
+    ritz32 = !ext || ext->ritz_estimate != BBJD_RITZ_FP64;
+    rq_lus = rq_fallbacks = 0;
+    if (ritz32) {
+        hC32.resize((size_t)maxsub * maxsub);
+        w32.resize(maxsub);
+        tau32.resize(maxsub);
+        zwork32.resize(64 * (size_t)maxsub + 64);
+        rwork32.resize(2 * (size_t)maxsub);
+    }
     return BBJD_SUCCESS;
 }
 
@@ -546,14 +568,26 @@ int Engine::solve_projected_schur(int k, int nkeep, bool reorder, int *target_po
     hH_k = k;
     auto t1 = std::chrono::steady_clock::now();
     qz_split[0] += std::chrono::duration<double>(t1 - t0).count();
-    auto to_lambda = [&](int i) {
-        const zc w = omega[i];
-        if (std::abs(w) < 1e-300 * std::abs(nu0)) { alpha[i] = 1.0; beta[i] = 0.0; return; }
-        alpha[i] = (1.0 / w - mu0) / nu0;
-        beta[i] = 1.0;
-    };
     const int lw = (int)zwork.size();
     const MklLapack &mkl = mkl_lapack();
+    if (!reorder && ritz32) {
+        // Between restarts the eigenvalues only rank the candidates: FP32
+        // estimates, the winner refined to an FP64 eigenpair of H.
+        const bool ok = eigenvalues32(k);
+        auto t3 = std::chrono::steady_clock::now();
+        if (ok)
+            for (int i = 0; i < k; ++i) to_lambda(i);
+        if (ok && refine_target(k, target_pos)) {
+            ritz_ready = true;
+            schur_step = true;
+            auto t4 = std::chrono::steady_clock::now();
+            qz_split[2] += std::chrono::duration<double>(t3 - t1).count();
+            qz_split[3] += std::chrono::duration<double>(t4 - t3).count();
+            qz_seconds += std::chrono::duration<double>(t4 - t0).count();
+            return 0;
+        }
+        rq_fallbacks++;                  // the FP64 path below; T (= H) is intact
+    }
     if (!reorder && mkl.zgeev && !g_concurrent_solve) {
         // Between restarts only the eigenvalues and the target's eigenvector
         // are used: eigenvalues by ZGEEV on a copy of H (no vectors), the
@@ -714,6 +748,140 @@ void Engine::dense_eigvec(int k, zc w, zc *x) {
     for (int j = 0; j < k; ++j)
         for (int i = j + 1; i < k; ++i) x[i] -= U[i + j * ld] * x[j];
     back_solve(x);
+}
+
+// lambda = (1 / omega - mu0) / nu0 of position i into alpha[i] / beta[i]
+// (beta = 0: omega = 0, an infinite lambda).
+void Engine::to_lambda(int i) {
+    const zc w = omega[i];
+    if (std::abs(w) < 1e-300 * std::abs(nu0)) {
+        alpha[i] = 1.0;
+        beta[i] = 0.0;
+        return;
+    }
+    alpha[i] = (1.0 / w - mu0) / nu0;
+    beta[i] = 1.0;
+}
+
+// FP32 estimates of the k eigenvalues of H (= ws->SA, ld maxsub) into
+// omega.  H is scaled by a power of two (exact) so that its largest
+// component lies in [0.5, 1): no FP32 overflow.  CGEEV from MKL when it is
+// loaded and the solve runs alone, else OpenBLAS's CGEHRD + CHSEQR.  false
+// for a zero or non-finite H or a LAPACK failure.
+bool Engine::eigenvalues32(int k) {
+    const size_t L = maxsub;
+    const zc *H = ws->SA;
+    double amax = 0.0;
+    for (int j = 0; j < k; ++j)
+        for (int i = 0; i < k; ++i) {
+            const zc h = H[i + j * L];
+            const double a = std::max(std::abs(h.real()), std::abs(h.imag()));
+            if (!(a <= amax)) amax = a;              // a NaN sticks
+        }
+    if (!(amax > 0.0) || !std::isfinite(amax)) return false;
+    int e2 = 0;
+    std::frexp(amax, &e2);
+    const double sc = std::ldexp(1.0, -e2);
+    for (int j = 0; j < k; ++j)
+        for (int i = 0; i < k; ++i) {
+            const zc h = H[i + j * L] * sc;
+            hC32[i + j * L] = std::complex<float>((float)h.real(), (float)h.imag());
+        }
+    const int bk = k, ld = (int)maxsub, one = 1;
+    int info = 0;
+    const MklLapack &mkl = mkl_lapack();
+    if (mkl.cgeev && !g_concurrent_solve) {
+        const int prev = mkl.set_local_threads(1);
+        const int lwork = std::min<int>((int)zwork32.size(), std::max(8 * k, 64));
+        mkl.cgeev("N", "N", &bk, hC32.data(), &ld, w32.data(), nullptr, &one, nullptr, &one,
+                  zwork32.data(), &lwork, rwork32.data(), &info);
+        mkl.set_local_threads(prev);
+    } else {
+        const int lw = (int)zwork32.size();
+        scipy_cgehrd_(&bk, &one, &bk, hC32.data(), &ld, tau32.data(), zwork32.data(), &lw, &info);
+        if (info) return false;
+        for (int j = 0; j < k; ++j)
+            for (int i = j + 2; i < k; ++i) hC32[i + j * L] = 0.0f;
+        std::complex<float> z1;
+        scipy_chseqr_("E", "N", &bk, &one, &bk, hC32.data(), &ld, w32.data(), &z1, &one,
+                      zwork32.data(), &lw, &info);
+    }
+    if (info) return false;
+    for (int i = 0; i < k; ++i) {
+        omega[i] = zc(w32[i].real(), w32[i].imag()) / sc;
+        if (!std::isfinite(omega[i].real()) || !std::isfinite(omega[i].imag())) return false;
+    }
+    return true;
+}
+
+// Rayleigh-quotient iteration on H (= ws->SA) from the estimate w: an
+// inverse-iteration eigenvector at the current shift (dense_eigvec), then
+// w = x^H H x / x^H x, until ||H x - w x|| <= 16 k eps ||H||_1 ||x|| (the
+// backward error of an FP64 eigensolver).  At most five factorisations;
+// false if the residual is still above the bound.
+bool Engine::rq_refine(int k, zc &w, zc *x) {
+    const size_t L = maxsub;
+    const zc *H = ws->SA;
+    double hnorm = 0.0;
+    for (int j = 0; j < k; ++j) {
+        double c = 0.0;
+        for (int i = 0; i < k; ++i) c += std::abs(H[i + j * L]);
+        hnorm = std::max(hnorm, c);
+    }
+    const double bound = 16.0 * k * DBL_EPSILON * std::max(hnorm, 1e-300);
+    std::vector<zc> &y = hys;
+    for (int it = 0; it < 5; ++it) {
+        dense_eigvec(k, w, x);
+        rq_lus++;
+        std::fill(y.begin(), y.begin() + k, zc(0.0));
+        for (int j = 0; j < k; ++j) {
+            const zc xj = x[j];
+            for (int i = 0; i < k; ++i) y[i] += H[i + j * L] * xj;
+        }
+        zc num = 0.0;
+        double den = 0.0;
+        for (int i = 0; i < k; ++i) {
+            num += std::conj(x[i]) * y[i];
+            den += std::norm(x[i]);
+        }
+        if (!(den > 0.0)) return false;
+        const zc wn = num / den;
+        double r2 = 0.0;
+        for (int i = 0; i < k; ++i) r2 += std::norm(y[i] - wn * x[i]);
+        w = wn;
+        if (std::sqrt(r2 / den) <= bound) return true;
+    }
+    return false;
+}
+
+// The target scan of select_and_scan over the FP32 estimates; the winner
+// is refined (rq_refine) and tested against the locked values again with
+// its FP64 value.  A winner that turns out locked is passed over for the
+// next candidate.  false when none is left or a refinement fails.
+bool Engine::refine_target(int k, int *target_pos) {
+    std::vector<char> skip(k, 0);
+    for (int attempt = 0; attempt < 8; ++attempt) {
+        int tpos = -1;
+        double best = DBL_MAX;
+        for (int i = 0; i < k; ++i) {
+            if (skip[i] || std::abs(beta[i]) < 1e-300) continue;
+            const zc lam = alpha[i] / beta[i];
+            if (is_locked(lam)) continue;
+            const double v = target_value(lam, sigma, target);
+            if (v < best) { best = v; tpos = i; }
+        }
+        if (tpos < 0) return false;
+        zc w = omega[tpos];
+        if (!rq_refine(k, w, hx.data())) return false;
+        omega[tpos] = w;
+        to_lambda(tpos);
+        if (std::abs(beta[tpos]) >= 1e-300 && !is_locked(alpha[tpos] / beta[tpos])) {
+            *target_pos = tpos;
+            return true;
+        }
+        skip[tpos] = 1;
+    }
+    return false;
 }
 
 // Eigenvector x of H = Q Hh Q^H for its eigenvalue w, where ZGEHRD left the

@@ -6,6 +6,7 @@
                                 [--inner-maxiter 0] [--inner-tol 1e-2]
                                 [--projected auto|qz|schur] [--lock robust|reference]
                                 [--precision fp64|mixed] [--verbose 0|1|2]
+                                [--ritz-estimate auto|fp64|fp32]
     python -m bbjd_b200.profile --sweep 32 [--threads 16] [--maxiter 2000]
 
 Builds the seeded pencil, uploads it, factors the exact LU (or the block
@@ -66,6 +67,7 @@ def main(argv=None):
     ap.add_argument("--inner-tol", type=float, default=1e-2)
     ap.add_argument("--verbose", type=int, default=0)
     ap.add_argument("--lock", default="robust", choices=["robust", "reference"])
+    ap.add_argument("--ritz-estimate", default="auto", choices=["auto", "fp64", "fp32"])
     a = ap.parse_args(argv)
     if a.sweep:
         return sweep(a.sweep, a.threads, a.precision, a.maxiter)
@@ -77,12 +79,13 @@ def main(argv=None):
                        minsub=a.minsub, inner_maxiter=a.inner_maxiter, inner_tol=a.inner_tol,
                        preconditioner=pc, v0=start_vector(P.n, 1), verbose=a.verbose,
                        return_info=True, timing=True, projected=a.projected, lock=a.lock,
-                       precision=a.precision)
+                       precision=a.precision, ritz_estimate=a.ritz_estimate)
     wall = time.time() - t0
     d = info["device"]
     print(f"n={P.n} iters={info['iters']} nconv={info['nconv']} wall={wall:.2f}s "
           f"host_qz={d['seconds_qz']:.2f}s device={d['seconds_device']:.2f}s "
-          f"launches={d['kernel_launches']} factor={pc.factor_seconds:.3f}s")
+          f"launches={d['kernel_launches']} factor={pc.factor_seconds:.3f}s "
+          f"refinement_lus={d['ritz_refinements']} fp64_fallbacks={d['ritz_fallbacks']}")
     for name, v in d["kernels"].items():
         if v["calls"]:
             print(f"  {name:8s} calls {v['calls']:6d}  ms {v['ms']:9.2f}  "

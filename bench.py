@@ -235,7 +235,8 @@ def run_ours(args):
     gen_s = time.time() - t0
     solve_kw = dict(k=w["k"], sigma=w["sigma"], tol=w["tol"], maxiter=w["maxiter"],
                     maxsub=w["maxsub"], minsub=w["minsub"], v0=v0, return_info=True,
-                    projected=args.projected, precision=args.precision)
+                    projected=args.projected, precision=args.precision,
+                    ritz_estimate=args.ritz_estimate)
     dims = dict(b=w["b"], nblk=w["nblk"], t=w["t"])
     dev = DevicePencil(arrays=pinned, **dims)
     pc = DevicePreconditioner(dev, w["sigma"], "exact", precision=args.precision)
@@ -321,7 +322,8 @@ def run_ours(args):
         "vs_baseline": None, "dtype": "complex128" if args.precision == "fp64" else "complex128+complex64",
         "data": "synthetic",
         "config": {"workload": WORKLOAD_NAME, **WORKLOAD, "precision": args.precision,
-                   "projected": args.projected, "preconditioner": "exact block-bordered LU (device)",
+                   "projected": args.projected, "ritz_estimate": args.ritz_estimate,
+                   "preconditioner": "exact block-bordered LU (device)",
                    "l2": "inputs larger than L2 (4.1 GB pencil), no flush"},
         "e2e": {"value": e_pairs_all / e_secs_max, "unit": "eigenpairs/s",
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
@@ -333,6 +335,8 @@ def run_ours(args):
                    "seconds_device_timed": round(d["seconds_device"], 3),
                    "factor_s": round(factor_s, 3), "setup_s": round(gen_s, 1),
                    "dgks_passes": d["dgks_passes"], "restarts": d["restarts"],
+                   "ritz_refinement_lus": d["ritz_refinements"],
+                   "ritz_fp64_fallbacks": d["ritz_fallbacks"],
                    "device_GB": round(d["bytes_device"] / 1e9, 1), "kernels": kern},
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -363,6 +367,9 @@ def main():
     ap.add_argument("--projected", default="auto", choices=["auto", "qz", "schur"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
                     help="fp64: the plain FP64 form; mixed: complex64 LU factors and first CGS pass")
+    ap.add_argument("--ritz-estimate", default="auto", choices=["auto", "fp64", "fp32"],
+                    help="projected eigenvalues between restarts: fp32 estimates + FP64 "
+                         "refinement of the target (auto), or all in fp64")
     ap.add_argument("--ref-iters", type=int, default=6,
                     help="reference outer iterations per CPU sample step")
     ap.add_argument("--no-cpu-baseline", action="store_true")

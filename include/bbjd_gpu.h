@@ -59,6 +59,17 @@ enum { BBJD_LOCK_ROBUST = 0, BBJD_LOCK_REFERENCE = 1 };
 /* Layout of result->eigenvectors from a device solve. */
 enum { BBJD_EVEC_COLUMN_MAJOR = 0, BBJD_EVEC_ROW_MAJOR = 1 };
 
+/* How the harmonic Schur-form projected solve picks the target between
+ * restarts (bbjd_device_ext.ritz_estimate).  FP64: the k projected
+ * eigenvalues in FP64, the target's eigenvector by inverse iteration.
+ * FP32: the k eigenvalues in complex64 (about half the host time), used only
+ * to rank the candidates; the chosen one is refined in FP64 by Rayleigh-
+ * quotient iteration on the FP64 projected matrix until its residual is
+ * 16 k eps ||H||_1, re-checked against the locked values, and the FP64 path
+ * runs whenever a refinement does not converge.  Returned eigenvalues,
+ * residuals and the convergence test are FP64 either way.  AUTO = FP32. */
+enum { BBJD_RITZ_AUTO = 0, BBJD_RITZ_FP64 = 1, BBJD_RITZ_FP32 = 2 };
+
 enum { BBJD_PC_NONE = 0, BBJD_PC_BBT_LU = 1, BBJD_PC_BLOCK_JACOBI = 2 };
 
 /* Copy a BBT pencil to the current device.  from_host = 1: pointers are host
@@ -109,6 +120,7 @@ typedef struct {
                                    Python caller returns, transposed on the
                                    device at the end of the solve (saves the
                                    host an O(n nconv) strided copy)          */
+    int     ritz_estimate;      /* BBJD_RITZ_AUTO (default), _FP64 or _FP32     */
     /* out */
     double  seconds_total;      /* wall time of the solve                       */
     double  seconds_qz;         /* host projected QZ + reorder                  */
@@ -119,6 +131,9 @@ typedef struct {
     int64_t dgks_passes;        /* second CGS passes taken                      */
     int64_t restarts;
     int64_t duplicates;         /* re-converged locked pairs not returned again */
+    int64_t ritz_refinements;   /* FP64 LU factorisations of the FP32 target
+                                   refinement (BBJD_RITZ_FP32)                */
+    int64_t ritz_fallbacks;     /* FP32 estimates replaced by the FP64 path    */
     double  kernel_ms[8];       /* per kernel class: spmv, orth, pencil, ritz,
                                    precond, restart, small, gmres (if timed)    */
     double  kernel_bytes[8];

@@ -34,17 +34,24 @@ def _check_pairs(P, ev, evecs, g, tol=1e-10):
     assert_no_duplicates(ev)
 
 
-@pytest.mark.parametrize("projected", ["qz", "schur"])
+@pytest.mark.parametrize("projected,ritz", [("qz", "auto"), ("schur", "fp32"), ("schur", "fp64")])
 @pytest.mark.parametrize("name", ["bbt_n516", "bbt_n1056_b32", "bbt_n4104"])
-def test_device_jdqz_matches_reference(name, projected):
+def test_device_jdqz_matches_reference(name, projected, ritz):
     g = _load(name)
     P = make_pencil(int(g["b"]), int(g["nblk"]), int(g["t"]), seed=int(g["seed"]))
     sigma = complex(g["sigma"])
     ev, evecs, info = jdqz(P, k=int(g["k"]), sigma=sigma, tol=1e-10, maxiter=int(g["maxiter"]),
                            maxsub=int(g["maxsub"]), minsub=int(g["minsub"]),
                            preconditioner="exact", v0=start_vector(P.n, int(g["seed"]) + 1),
-                           return_info=True, projected=projected)
+                           return_info=True, projected=projected, ritz_estimate=ritz,
+                           timing=True)
     assert info["nconv"] == int(g["k"]) and info["status"] == 0
+    d = info["device"]
+    if projected == "schur" and ritz == "fp32":
+        # FP32 estimates ranked the candidates and were refined in FP64
+        assert d["ritz_refinements"] > 0
+    else:
+        assert d["ritz_refinements"] == 0 and d["ritz_fallbacks"] == 0
     _check_pairs(P, ev, evecs, g)
     # same eigenvalues as the reference's own run
     assert match_set(ev, g["eigenvalues"]).max() < EIG_ATOL
