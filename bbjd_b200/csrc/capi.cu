@@ -446,11 +446,8 @@ bbjd_status bbjd_dev_orthogonalize(bbjd_int n, bbjd_int k, const bbjd_zomplex *Q
                    dv, S.scal, nullptr, nullptr, nullptr, nullptr, st);
     } else {
         s = tsdot(S, 1, 1, (int)k, ldq, dQ, nullptr, dv, nullptr, S.red, nullptr, st);
-        if (!s) s = update(S, (int)k, ldq, dQ, S.red, nullptr, mk(1, 0), mk(0, 0), mk(1, 0), dv, mk(0, 0),
-                           nullptr, dv, S.scal, S.red + k, nullptr, S.flags, nullptr, st);
-        if (!s) s = tsdot(S, 1, 1, (int)k, ldq, dQ, nullptr, dv, nullptr, S.red + S.maxX, S.flags, st);
-        if (!s) s = update(S, (int)k, ldq, dQ, S.red + S.maxX, nullptr, mk(1, 0), mk(0, 0), mk(1, 0), dv,
-                           mk(0, 0), nullptr, dv, S.scal, nullptr, nullptr, nullptr, S.flags, st);
+        if (!s) s = cgs_tail(S, (int)k, ldq, dQ, S.red, nullptr, mk(1, 0), mk(0, 0), mk(1, 0), dv, mk(0, 0),
+                             nullptr, dv, S.scal, S.red + k, nullptr, S.flags, S.red + S.maxX, st);
     }
     double nrm = 0.0;
     int flag = 0;

@@ -209,6 +209,149 @@ __global__ void __launch_bounds__(256) k_update(
     }
 }
 
+// ---------------------------------------------------------------------------
+// A CGS update fused with the dots of the DGKS re-pass that may follow it:
+// v_out, ||v_out|| and the DGKS flag exactly as k_update, and, from the same
+// read of Q, per-CTA partials of Q^H v_out (partial[g][j], j < ncols;
+// partial[g][ncols] = the CTA's ||v_out||^2) for k_reduce.  Without it the
+// re-pass reads Q twice more (dots, then the update); with it once.
+//
+// One persistent CTA of 16 warps per SM walks tiles of 32 rows.  A tile's
+// 32 x ncols slice of Q is copied to shared memory by cp.async, double-
+// buffered (the next tile is in flight while this one is used).  Warp w
+// owns columns w, w + 16, ... and lane l row l of the tile: the warps'
+// partial sums of Q h meet in shared memory, warp 0 forms v_out for the 32
+// rows (it alone reads v_in and writes v_out, which may alias), and every
+// lane accumulates conj(Q) v_out for its columns in registers across tiles;
+// the warp sums happen once, at the end.  Summation orders are fixed.
+constexpr int UD_TR = 32;          // rows per tile (lane = row)
+constexpr int UD_WARPS = 16;
+constexpr int UD_CPW = 14;         // columns per warp: ncols <= 224
+constexpr size_t UD_SMEM_LIMIT = 231424;
+
+static size_t update_dot_smem(int ncols) {
+    return sizeof(cplx) * ((size_t)2 * ncols * UD_TR + ncols + UD_WARPS * UD_TR + UD_TR);
+}
+
+bool update_dot_fits(int ncols) {
+    return ncols >= 1 && ncols <= UD_WARPS * UD_CPW && update_dot_smem(ncols) <= UD_SMEM_LIMIT;
+}
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem, int src_bytes) {
+    const unsigned a = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(a), "l"(gmem), "r"(src_bytes)
+                 : "memory");
+}
+
+__global__ void __launch_bounds__(UD_WARPS * 32, 1) k_update_dot(
+    int64_t n, int ncols, int64_t ld, const cplx *__restrict__ Q, const cplx *__restrict__ h1,
+    const cplx *__restrict__ h2, cplx c1, cplx c2, cplx a, const cplx *v_in, cplx b,
+    const cplx *w_in, cplx *v_out, cplx *__restrict__ partial, double *__restrict__ nrm_part,
+    unsigned *counter, double *norm_out, const cplx *ref_nsq, const double *ref_nrm,
+    int *flag_out) {
+    extern __shared__ cplx ud_smem[];
+    const int per = ncols * UD_TR;
+    cplx *Qs = ud_smem;                         // two tiles, [ncols][UD_TR] each
+    cplx *hs = Qs + 2 * per;                    // c1 h1 + c2 h2
+    cplx *red = hs + ncols;                     // [UD_WARPS][UD_TR] partial sums of Q h
+    cplx *vs = red + UD_WARPS * UD_TR;          // the tile's v_out
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    for (int j = tid; j < ncols; j += blockDim.x) {
+        cplx h = cmul(c1, h1[j]);
+        if (h2) cfma(h, c2, h2[j]);
+        hs[j] = h;
+    }
+    const int64_t ntiles = (n + UD_TR - 1) / UD_TR;
+    // rows past n are zero-filled (source size 0), so they add nothing
+    auto issue = [&](int64_t tile, cplx *dst) {
+        const int64_t row0 = tile * UD_TR;
+        for (int e = tid; e < per; e += blockDim.x) {
+            const int j = e >> 5, r = e & 31;
+            const int64_t row = row0 + r;
+            const bool in = row < n;
+            cp_async16(dst + e, Q + (int64_t)j * ld + (in ? row : 0), in ? 16 : 0);
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    };
+    cplx acc[UD_CPW];
+#pragma unroll
+    for (int c = 0; c < UD_CPW; ++c) acc[c] = mk(0.0, 0.0);
+    double nsq = 0.0;
+    int buf = 0;
+    int64_t tile = blockIdx.x;
+    if (tile < ntiles) issue(tile, Qs);
+    for (; tile < ntiles; tile += gridDim.x) {
+        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+        __syncthreads();                        // tile landed; the other buffer is free
+        const int64_t next = tile + gridDim.x;
+        if (next < ntiles) issue(next, Qs + (buf ^ 1) * per);
+        const cplx *Qt = Qs + buf * per;
+        const int64_t row = tile * UD_TR + lane;
+        cplx base = mk(0.0, 0.0);
+        if (warp == 0 && row < n) {
+            if (v_in) base = cmul(a, v_in[row]);
+            if (w_in) cfma(base, b, w_in[row]);
+        }
+        cplx p = mk(0.0, 0.0);
+#pragma unroll
+        for (int c = 0; c < UD_CPW; ++c) {
+            const int j = warp + UD_WARPS * c;
+            if (j < ncols) cfma(p, Qt[j * UD_TR + lane], hs[j]);
+        }
+        red[warp * UD_TR + lane] = p;
+        __syncthreads();
+        if (warp == 0) {
+            cplx sum = red[lane];
+            for (int w = 1; w < UD_WARPS; ++w) sum = cadd(sum, red[w * UD_TR + lane]);
+            const cplx vo = row < n ? csub(base, sum) : mk(0.0, 0.0);
+            vs[lane] = vo;
+            if (row < n) {
+                v_out[row] = vo;
+                nsq += cabs2(vo);
+            }
+        }
+        __syncthreads();
+        const cplx vo = vs[lane];
+#pragma unroll
+        for (int c = 0; c < UD_CPW; ++c) {
+            const int j = warp + UD_WARPS * c;
+            if (j < ncols) cfmac(acc[c], Qt[j * UD_TR + lane], vo);
+        }
+        buf ^= 1;
+    }
+    cplx *out = partial + (int64_t)blockIdx.x * (ncols + 1);
+#pragma unroll
+    for (int c = 0; c < UD_CPW; ++c) {
+        const int j = warp + UD_WARPS * c;
+        const cplx sum = warp_sum(acc[c]);
+        if (lane == 0 && j < ncols) out[j] = sum;
+    }
+    __shared__ bool last;
+    if (warp == 0) {
+        const double t = warp_sum(nsq);
+        if (lane == 0) {
+            out[ncols] = mk(t, 0.0);
+            nrm_part[blockIdx.x] = t;
+            __threadfence();
+            last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+        }
+    }
+    __syncthreads();
+    if (!last || warp != 0) return;
+    double t = 0.0;
+    for (int g = lane; g < (int)gridDim.x; g += 32) t += __ldcg(nrm_part + g);
+    t = warp_sum(t);
+    if (lane == 0) {
+        const double nrm = sqrt(t);
+        *norm_out = nrm;
+        if (flag_out) {
+            const double before = ref_nsq ? sqrt(ref_nsq->x) : (ref_nrm ? *ref_nrm : 0.0);
+            *flag_out = (nrm < 0.7071 * before) ? 1 : 0;
+        }
+        *counter = 0u;
+    }
+}
+
 // out = v / norm (norm read on the device); if norm <= thresh, out = v.
 __global__ void k_scale(int64_t n, const cplx *v, const double *norm, double thresh, cplx *out) {
     const double nr = *norm;
@@ -468,6 +611,42 @@ bbjd_status update(Scratch &S, int ncols, int64_t ld, const cplx *Q, const cplx 
                                       flag_in);
     BBJD_LAUNCH_CHECK();
     return BBJD_SUCCESS;
+}
+
+bbjd_status cgs_tail(Scratch &S, int ncols, int64_t ld, const cplx *Q, const cplx *h1,
+                     const cplx *h2, cplx c1, cplx c2, cplx a, const cplx *v_in, cplx b,
+                     const cplx *w_in, cplx *v_out, double *norm_out, const cplx *ref_nsq,
+                     const double *ref_nrm, int *flag, cplx *h_re, cudaStream_t st) {
+    bbjd_status s;
+    if (ncols > 0 && update_dot_fits(ncols) && ncols + 1 <= S.maxX) {
+        static std::once_flag once;
+        static cudaError_t attr = cudaSuccess;
+        std::call_once(once, [] {
+            attr = cudaFuncSetAttribute(k_update_dot, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)UD_SMEM_LIMIT);
+        });
+        if (attr != cudaSuccess) {
+            set_last_error(attr, "cudaFuncSetAttribute(k_update_dot)", __FILE__, __LINE__);
+            return BBJD_ERR_CUDA;
+        }
+        const int64_t ntiles = (S.n + UD_TR - 1) / UD_TR;
+        const int G = (int)std::max<int64_t>(1, std::min<int64_t>({(int64_t)num_sms(), ntiles,
+                                                                    (int64_t)S.G}));
+        k_update_dot<<<G, UD_WARPS * 32, update_dot_smem(ncols), st>>>(
+            S.n, ncols, ld, Q, h1, h2, c1, c2, a, v_in, b, w_in, v_out, S.partial, S.nrm_part,
+            S.counter, norm_out, ref_nsq, ref_nrm, flag);
+        BBJD_LAUNCH_CHECK();
+        k_reduce<<<(ncols + 1 + 31) / 32, 256, 0, st>>>(S.partial, G, ncols + 1, h_re, flag);
+        BBJD_LAUNCH_CHECK();
+    } else {
+        if ((s = update(S, ncols, ld, Q, h1, h2, c1, c2, a, v_in, b, w_in, v_out, norm_out, ref_nsq,
+                        ref_nrm, flag, nullptr, st)))
+            return s;
+        if (ncols == 0) return BBJD_SUCCESS;
+        if ((s = tsdot(S, 1, 1, ncols, ld, Q, nullptr, v_out, nullptr, h_re, flag, st))) return s;
+    }
+    return update(S, ncols, ld, Q, h_re, nullptr, mk(1, 0), mk(0, 0), mk(1, 0), v_out, mk(0, 0),
+                  nullptr, v_out, norm_out, nullptr, nullptr, nullptr, flag, st);
 }
 
 bbjd_status scale_by_norm(Scratch &S, const cplx *v, const double *norm, double thresh,

@@ -39,6 +39,17 @@ bbjd_status update(Scratch &S, int ncols, int64_t ld, const cplx *Q, const cplx 
                    const cplx *w_in, cplx *v_out, double *norm_out, const cplx *ref_nsq,
                    const double *ref_nrm, int *flag_out, const int *flag_in, cudaStream_t st);
 
+// The rest of a CGS2 / DGKS step once the first pass's dots h1 (and h2) are
+// known: v_out = a v_in + b w_in - Q (c1 h1 + c2 h2), ||v_out|| into
+// *norm_out and the DGKS flag into *flag (as update()); then, where the
+// flag is raised, h_re = Q^H v_out and v_out -= Q h_re, ||v_out||.  For
+// ncols within update_dot_fits() the re-pass dots come from the update's
+// own read of Q (one pass over Q fewer).  h_re holds ncols + 1 values.
+bool update_dot_fits(int ncols);
+bbjd_status cgs_tail(Scratch &S, int ncols, int64_t ld, const cplx *Q, const cplx *h1,
+                     const cplx *h2, cplx c1, cplx c2, cplx a, const cplx *v_in, cplx b,
+                     const cplx *w_in, cplx *v_out, double *norm_out, const cplx *ref_nsq,
+                     const double *ref_nrm, int *flag, cplx *h_re, cudaStream_t st);
 bbjd_status scale_by_norm(Scratch &S, const cplx *v, const double *norm, double thresh,
                           cplx *out, cudaStream_t st);
 bbjd_status axpby(Scratch &S, const cplx *a_dev, cplx a, const cplx *x, const cplx *b_dev, cplx b,

@@ -257,9 +257,12 @@ void Engine::release() {
     st = nullptr;
 }
 
-// A DGKS re-pass ran (the device flag was read back): count its traffic.
+// A DGKS re-pass ran (the device flag was read back): count its traffic --
+// its update alone (one read of Q, v read and written) when its dots came
+// from the first pass's update (cgs_tail), else a dot pass and an update.
 void Engine::second_pass_bytes(int cls, int k) {
-    const double b = 16.0 * (double)n * (2.0 * k + 3.0);
+    const double b = update_dot_fits(k) ? 16.0 * (double)n * (k + 2.0)
+                                        : 16.0 * (double)n * (2.0 * k + 3.0);
     T.bytes[cls] += b;
     bytes_dev += b;
 }
@@ -307,15 +310,9 @@ bbjd_status Engine::orthogonalize(const cplx *Q, int64_t ldq, int k, cplx *v, do
     cplx *h = S.red;
     s = tsdot(S, 1, 1, k, ldq, Q, nullptr, v, nullptr, h, nullptr, st);
     if (s) return s;
-    s = update(S, k, ldq, Q, h, nullptr, mk(1, 0), mk(0, 0), mk(1, 0), v, mk(0, 0), nullptr, v,
-               norm_dev, h + k, nullptr, flag, nullptr, st);
-    if (s) return s;
-    // second pass, executed only when the device raised the DGKS flag
-    cplx *h2 = S.red + S.maxX;
-    s = tsdot(S, 1, 1, k, ldq, Q, nullptr, v, nullptr, h2, flag, st);
-    if (s) return s;
-    s = update(S, k, ldq, Q, h2, nullptr, mk(1, 0), mk(0, 0), mk(1, 0), v, mk(0, 0), nullptr, v,
-               norm_dev, nullptr, nullptr, nullptr, flag, st);
+    // update, DGKS test, and the second pass where the device raised the flag
+    s = cgs_tail(S, k, ldq, Q, h, nullptr, mk(1, 0), mk(0, 0), mk(1, 0), v, mk(0, 0), nullptr, v,
+                 norm_dev, h + k, nullptr, flag, S.red + S.maxX, st);
     T.end();
     bytes_dev += pass_bytes;
     return s;
@@ -336,13 +333,8 @@ bbjd_status Engine::orthogonalize_mixed(int k, cplx *v, double *norm_dev) {
     int *flag = dflag + FL_T;
     cplx *h = S.red;
     if ((s = tsdot(S, 1, 1, k, n, V, nullptr, v, nullptr, h, nullptr, st))) return s;
-    if ((s = update(S, k, n, V, h, nullptr, mk(1, 0), mk(0, 0), mk(1, 0), v, mk(0, 0), nullptr, v,
-                    norm_dev, nullptr, dscal + SC_TMP2, flag, nullptr, st)))
-        return s;
-    cplx *h2 = S.red + S.maxX;
-    if ((s = tsdot(S, 1, 1, k, n, V, nullptr, v, nullptr, h2, flag, st))) return s;
-    if ((s = update(S, k, n, V, h2, nullptr, mk(1, 0), mk(0, 0), mk(1, 0), v, mk(0, 0), nullptr, v,
-                    norm_dev, nullptr, nullptr, nullptr, flag, st)))
+    if ((s = cgs_tail(S, k, n, V, h, nullptr, mk(1, 0), mk(0, 0), mk(1, 0), v, mk(0, 0), nullptr, v,
+                      norm_dev, nullptr, dscal + SC_TMP2, flag, S.red + S.maxX, st)))
         return s;
     T.end();
     bytes_dev += b1 + 16.0 * (double)n * (2.0 * k + 3.0);
@@ -1386,13 +1378,9 @@ bbjd_status Engine::run() {
             return s;
         cplx *hAB = xdev;  // [hA (k) | hB (k) | norms]
         if ((s = tsdot(S, 1, 2, (int)k, ld, W, nullptr, AVk, BVk, hAB, nullptr, st))) return s;
-        if ((s = update(S, (int)k, ld, W, hAB, hAB + k, C(nu0), C(mu0), mk(1, 0), wnew, mk(0, 0), nullptr,
-                        wnew, dscal + SC_WNORM, nullptr, dscal + SC_WPRE, dflag + FL_W, nullptr, st)))
-            return s;
-        cplx *h2 = S.red + S.maxX;
-        if ((s = tsdot(S, 1, 1, (int)k, ld, W, nullptr, wnew, nullptr, h2, dflag + FL_W, st))) return s;
-        if ((s = update(S, (int)k, ld, W, h2, nullptr, mk(1, 0), mk(0, 0), mk(1, 0), wnew, mk(0, 0), nullptr,
-                        wnew, dscal + SC_WNORM, nullptr, nullptr, nullptr, dflag + FL_W, st)))
+        if ((s = cgs_tail(S, (int)k, ld, W, hAB, hAB + k, C(nu0), C(mu0), mk(1, 0), wnew, mk(0, 0),
+                          nullptr, wnew, dscal + SC_WNORM, nullptr, dscal + SC_WPRE, dflag + FL_W,
+                          S.red + S.maxX, st)))
             return s;
         T.end();
         bytes_dev += 16.0 * n * (2.0 * k + 6.0);

@@ -113,12 +113,17 @@ def test_block_jacobi_matches_host(b, nblk, t):
     assert np.linalg.norm(_host(xd) - ref) / np.linalg.norm(ref) < 1e-12
 
 
-@pytest.mark.parametrize("n,k", [(1000, 0), (1000, 1), (4104, 37), (100003, 200), (50, 50)])
-def test_orthogonalize_matches_oracle(n, k):
+# k <= 214: the update and the re-pass dots share one read of Q (cgs_tail's
+# fused kernel); k = 215 takes the separate dot pass.  repass=False: v has no
+# large component along Q, so the DGKS flag stays down and the re-pass is skipped.
+@pytest.mark.parametrize("n,k,repass", [(1000, 0, True), (1000, 1, True), (4104, 37, True),
+                                        (100003, 200, True), (50, 50, True), (7001, 214, True),
+                                        (7001, 215, True), (70001, 120, False), (33, 5, False)])
+def test_orthogonalize_matches_oracle(n, k, repass):
     import torch
     rng = np.random.default_rng(n + k)
     Q = np.linalg.qr(rng.standard_normal((n, max(k, 1))) + 1j * rng.standard_normal((n, max(k, 1))))[0][:, :k]
-    v = _rand(n, 9) + (Q @ _rand(k, 8) * 1000 if k else 0)
+    v = _rand(n, 9) + (Q @ _rand(k, 8) * 1000 if k and repass else 0)
     Qd = _dev(np.asfortranarray(Q).T.copy()) if k else _dev(np.zeros(1, np.complex128))
     vd = _dev(v)
     nrm = C.c_double()
@@ -132,9 +137,9 @@ def test_orthogonalize_matches_oracle(n, k):
     assert np.linalg.norm(_host(vd) - vv) < 1e-12 * np.linalg.norm(v)
     if k:
         # the DGKS decision (reference jd_core.c:232) made on the device
-        # matches the host's: the large component along Q forces the re-pass
+        # matches the host's: a large component along Q forces the re-pass
         after1 = np.linalg.norm(v - Q @ (Q.conj().T @ v))
-        assert second.value == int(after1 < 0.7071 * np.linalg.norm(v)) == 1
+        assert second.value == int(after1 < 0.7071 * np.linalg.norm(v)) == int(repass)
         assert np.abs(Q.conj().T @ _host(vd)).max() < 1e-12 * np.linalg.norm(v)
 
 
