@@ -216,25 +216,28 @@ __global__ void __launch_bounds__(256) k_update(
 // partial[g][ncols] = the CTA's ||v_out||^2) for k_reduce.  Without it the
 // re-pass reads Q twice more (dots, then the update); with it once.
 //
-// One persistent CTA of 16 warps per SM walks tiles of 32 rows.  A tile's
-// 32 x ncols slice of Q is copied to shared memory by cp.async, double-
-// buffered (the next tile is in flight while this one is used).  Warp w
-// owns columns w, w + 16, ... and lane l row l of the tile: the warps'
-// partial sums of Q h meet in shared memory, warp 0 forms v_out for the 32
-// rows (it alone reads v_in and writes v_out, which may alias), and every
-// lane accumulates conj(Q) v_out for its columns in registers across tiles;
-// the warp sums happen once, at the end.  Summation orders are fixed.
-constexpr int UD_TR = 32;          // rows per tile (lane = row)
+// One persistent CTA of 16 warps per SM walks tiles of 16 rows.  A tile's
+// 16 x ncols slice of Q is copied to shared memory by cp.async into a ring
+// of four buffers, so three tiles are in flight while one is used (one
+// tile in flight left each SM waiting a full memory latency per tile).
+// Lane l of warp w serves row l & 15 of the tile and columns
+// w + 16 (2c + (l >> 4)), c = 0, 1, ...: the lanes' partial sums of Q h meet
+// in shared memory, warp 0 forms v_out for the 16 rows (it alone reads v_in
+// and writes v_out, which may alias), and every lane accumulates conj(Q)
+// v_out for its columns in registers across tiles; the sums over the 16
+// lanes of a column happen once, at the end.  Summation orders are fixed.
+constexpr int UD_TR = 16;          // rows per tile
+constexpr int UD_STAGES = 4;       // tiles in the shared-memory ring
 constexpr int UD_WARPS = 16;
-constexpr int UD_CPW = 14;         // columns per warp: ncols <= 224
+constexpr int UD_CPL = 7;          // columns per lane: ncols <= 2 * 16 * 7 = 224
 constexpr size_t UD_SMEM_LIMIT = 231424;
 
 static size_t update_dot_smem(int ncols) {
-    return sizeof(cplx) * ((size_t)2 * ncols * UD_TR + ncols + UD_WARPS * UD_TR + UD_TR);
+    return sizeof(cplx) * ((size_t)UD_STAGES * ncols * UD_TR + ncols + UD_WARPS * 32 + UD_TR);
 }
 
 bool update_dot_fits(int ncols) {
-    return ncols >= 1 && ncols <= UD_WARPS * UD_CPW && update_dot_smem(ncols) <= UD_SMEM_LIMIT;
+    return ncols >= 1 && ncols <= 2 * UD_WARPS * UD_CPL && update_dot_smem(ncols) <= UD_SMEM_LIMIT;
 }
 
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem, int src_bytes) {
@@ -251,80 +254,92 @@ __global__ void __launch_bounds__(UD_WARPS * 32, 1) k_update_dot(
     int *flag_out) {
     extern __shared__ cplx ud_smem[];
     const int per = ncols * UD_TR;
-    cplx *Qs = ud_smem;                         // two tiles, [ncols][UD_TR] each
-    cplx *hs = Qs + 2 * per;                    // c1 h1 + c2 h2
-    cplx *red = hs + ncols;                     // [UD_WARPS][UD_TR] partial sums of Q h
-    cplx *vs = red + UD_WARPS * UD_TR;          // the tile's v_out
+    cplx *Qs = ud_smem;                         // UD_STAGES tiles, [ncols][UD_TR] each
+    cplx *hs = Qs + UD_STAGES * per;            // c1 h1 + c2 h2
+    cplx *red = hs + ncols;                     // [UD_WARPS][32] partial sums of Q h
+    cplx *vs = red + UD_WARPS * 32;             // the tile's v_out
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int r = lane & 15, half = lane >> 4;
     for (int j = tid; j < ncols; j += blockDim.x) {
         cplx h = cmul(c1, h1[j]);
         if (h2) cfma(h, c2, h2[j]);
         hs[j] = h;
     }
     const int64_t ntiles = (n + UD_TR - 1) / UD_TR;
-    // rows past n are zero-filled (source size 0), so they add nothing
-    auto issue = [&](int64_t tile, cplx *dst) {
-        const int64_t row0 = tile * UD_TR;
-        for (int e = tid; e < per; e += blockDim.x) {
-            const int j = e >> 5, r = e & 31;
-            const int64_t row = row0 + r;
-            const bool in = row < n;
-            cp_async16(dst + e, Q + (int64_t)j * ld + (in ? row : 0), in ? 16 : 0);
+    // one commit group per call, empty past the last tile; rows past n are
+    // zero-filled (source size 0), so they add nothing
+    auto issue = [&](int64_t tile, int slot) {
+        if (tile < ntiles) {
+            const int64_t row0 = tile * UD_TR;
+            cplx *dst = Qs + slot * per;
+            for (int e = tid; e < per; e += blockDim.x) {
+                const int j = e >> 4, rr = e & 15;
+                const int64_t row = row0 + rr;
+                const bool in = row < n;
+                cp_async16(dst + e, Q + (int64_t)j * ld + (in ? row : 0), in ? 16 : 0);
+            }
         }
         asm volatile("cp.async.commit_group;\n" ::: "memory");
     };
-    cplx acc[UD_CPW];
+    cplx acc[UD_CPL];
 #pragma unroll
-    for (int c = 0; c < UD_CPW; ++c) acc[c] = mk(0.0, 0.0);
+    for (int c = 0; c < UD_CPL; ++c) acc[c] = mk(0.0, 0.0);
     double nsq = 0.0;
-    int buf = 0;
-    int64_t tile = blockIdx.x;
-    if (tile < ntiles) issue(tile, Qs);
-    for (; tile < ntiles; tile += gridDim.x) {
-        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-        __syncthreads();                        // tile landed; the other buffer is free
-        const int64_t next = tile + gridDim.x;
-        if (next < ntiles) issue(next, Qs + (buf ^ 1) * per);
-        const cplx *Qt = Qs + buf * per;
-        const int64_t row = tile * UD_TR + lane;
+    const int64_t G = gridDim.x;
+#pragma unroll
+    for (int s = 0; s < UD_STAGES - 1; ++s) issue(blockIdx.x + s * G, s);
+    int slot = 0;
+    for (int64_t tile = blockIdx.x; tile < ntiles; tile += G) {
+        asm volatile("cp.async.wait_group %0;\n" ::"n"(UD_STAGES - 2) : "memory");
+        __syncthreads();                        // this tile landed; the slot used last is free
+        issue(tile + (UD_STAGES - 1) * G, (slot + UD_STAGES - 1) % UD_STAGES);
+        const cplx *Qt = Qs + slot * per;
+        const int64_t row = tile * UD_TR + r;
         cplx base = mk(0.0, 0.0);
-        if (warp == 0 && row < n) {
+        if (warp == 0 && half == 0 && row < n) {
             if (v_in) base = cmul(a, v_in[row]);
             if (w_in) cfma(base, b, w_in[row]);
         }
         cplx p = mk(0.0, 0.0);
 #pragma unroll
-        for (int c = 0; c < UD_CPW; ++c) {
-            const int j = warp + UD_WARPS * c;
-            if (j < ncols) cfma(p, Qt[j * UD_TR + lane], hs[j]);
+        for (int c = 0; c < UD_CPL; ++c) {
+            const int j = warp + UD_WARPS * (2 * c + half);
+            if (j < ncols) cfma(p, Qt[j * UD_TR + r], hs[j]);
         }
-        red[warp * UD_TR + lane] = p;
+        red[warp * 32 + lane] = p;
         __syncthreads();
-        if (warp == 0) {
-            cplx sum = red[lane];
-            for (int w = 1; w < UD_WARPS; ++w) sum = cadd(sum, red[w * UD_TR + lane]);
+        if (warp == 0 && half == 0) {
+            cplx sum = cadd(red[r], red[r + 16]);
+            for (int w = 1; w < UD_WARPS; ++w) sum = cadd(sum, cadd(red[w * 32 + r], red[w * 32 + r + 16]));
             const cplx vo = row < n ? csub(base, sum) : mk(0.0, 0.0);
-            vs[lane] = vo;
+            vs[r] = vo;
             if (row < n) {
                 v_out[row] = vo;
                 nsq += cabs2(vo);
             }
         }
         __syncthreads();
-        const cplx vo = vs[lane];
+        const cplx vo = vs[r];
 #pragma unroll
-        for (int c = 0; c < UD_CPW; ++c) {
-            const int j = warp + UD_WARPS * c;
-            if (j < ncols) cfmac(acc[c], Qt[j * UD_TR + lane], vo);
+        for (int c = 0; c < UD_CPL; ++c) {
+            const int j = warp + UD_WARPS * (2 * c + half);
+            if (j < ncols) cfmac(acc[c], Qt[j * UD_TR + r], vo);
         }
-        buf ^= 1;
+        slot = (slot + 1) % UD_STAGES;
     }
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    // column sums over the 16 lanes of each half-warp
     cplx *out = partial + (int64_t)blockIdx.x * (ncols + 1);
 #pragma unroll
-    for (int c = 0; c < UD_CPW; ++c) {
-        const int j = warp + UD_WARPS * c;
-        const cplx sum = warp_sum(acc[c]);
-        if (lane == 0 && j < ncols) out[j] = sum;
+    for (int c = 0; c < UD_CPL; ++c) {
+        cplx v = acc[c];
+#pragma unroll
+        for (int o = 8; o > 0; o >>= 1) {
+            v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+            v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+        }
+        const int j = warp + UD_WARPS * (2 * c + half);
+        if (r == 0 && j < ncols) out[j] = v;
     }
     __shared__ bool last;
     if (warp == 0) {
