@@ -216,39 +216,28 @@ __global__ void __launch_bounds__(256) k_update(
 // partial[g][ncols] = the CTA's ||v_out||^2) for k_reduce.  Without it the
 // re-pass reads Q twice more (dots, then the update); with it once.
 //
-// One persistent CTA of 16 warps per SM walks tiles of TR rows (32 when
-// ncols <= 105, else 16).  A tile's TR x ncols slice of Q and its rows of
-// v_in and w_in are copied to shared memory by cp.async into a ring of four
-// buffers, so three tiles are in flight while one is used.  Lane l of warp
-// w serves row l % TR and columns w + 16 (H c + l / TR), H = 32 / TR,
-// c = 0, 1, ...; the lanes' partial sums of Q h meet in shared memory and
-// each row's 512 / TR partials are summed by a group of as many lanes (one
-// shuffle tree per row, all rows at once); the group's first lane forms
-// v_out for its row.  Every lane accumulates conj(Q) v_out for its columns
-// in registers across tiles; the sums over the TR lanes of a column happen
-// once, at the end.  Summation orders are fixed.
-constexpr int UD_STAGES = 4;       // tiles in the shared-memory ring
+// One persistent CTA of 16 warps per SM walks tiles of 32 rows.  A tile's
+// 32 x ncols slice of Q is copied to shared memory by cp.async, double-
+// buffered (the next tile is in flight while this one is used).  Warp w
+// owns columns w, w + 16, ... and lane l row l of the tile: the warps'
+// partial sums of Q h meet in shared memory, warp 0 forms v_out for the 32
+// rows (it alone reads v_in and writes v_out, which may alias), and every
+// lane accumulates conj(Q) v_out for its columns in registers across tiles;
+// the warp sums happen once, at the end.  Summation orders are fixed.
+constexpr int UD_TR = 32;          // rows per tile (lane = row)
 constexpr int UD_WARPS = 16;
-constexpr int UD_MAX_COLS = 224;   // 16 warps x 32 / TR lanes x 14 TR / 32 columns
+constexpr int UD_CPW = 14;         // columns per warp: ncols <= 224
 constexpr int UD_MIN_COLS = 64;    // below, the separate dot pass is as cheap
 constexpr size_t UD_SMEM_LIMIT = 231424;
 
-template <int TR>
 static size_t update_dot_smem(int ncols) {
-    return sizeof(cplx) * ((size_t)UD_STAGES * ncols * TR + (size_t)UD_STAGES * 2 * TR + ncols +
-                           UD_WARPS * 32 + TR) +
-           sizeof(double) * UD_WARPS;
+    return sizeof(cplx) * ((size_t)2 * ncols * UD_TR + ncols + UD_WARPS * UD_TR + UD_TR);
 }
 
-// rows per tile for ncols columns, 0 = the kernel does not take this size
-static int update_dot_rows(int ncols) {
-    if (ncols < UD_MIN_COLS || ncols > UD_MAX_COLS) return 0;
-    if (update_dot_smem<32>(ncols) <= UD_SMEM_LIMIT) return 32;
-    if (update_dot_smem<16>(ncols) <= UD_SMEM_LIMIT) return 16;
-    return 0;
+bool update_dot_fits(int ncols) {
+    return ncols >= UD_MIN_COLS && ncols <= UD_WARPS * UD_CPW &&
+           update_dot_smem(ncols) <= UD_SMEM_LIMIT;
 }
-
-bool update_dot_fits(int ncols) { return update_dot_rows(ncols) != 0; }
 
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem, int src_bytes) {
     const unsigned a = (unsigned)__cvta_generic_to_shared(smem);
@@ -256,134 +245,98 @@ __device__ __forceinline__ void cp_async16(void *smem, const void *gmem, int src
                  : "memory");
 }
 
-template <int TR>
 __global__ void __launch_bounds__(UD_WARPS * 32, 1) k_update_dot(
     int64_t n, int ncols, int64_t ld, const cplx *__restrict__ Q, const cplx *__restrict__ h1,
     const cplx *__restrict__ h2, cplx c1, cplx c2, cplx a, const cplx *v_in, cplx b,
     const cplx *w_in, cplx *v_out, cplx *__restrict__ partial, double *__restrict__ nrm_part,
     unsigned *counter, double *norm_out, const cplx *ref_nsq, const double *ref_nrm,
     int *flag_out) {
-    constexpr int H = 32 / TR;                       // column groups per warp
-    constexpr int CPL = UD_MAX_COLS / (UD_WARPS * H);  // columns per lane
-    constexpr int P = UD_WARPS * 32 / TR;            // partial sums per row
     extern __shared__ cplx ud_smem[];
-    const int per = ncols * TR;
-    cplx *Qs = ud_smem;                              // [UD_STAGES][ncols][TR]
-    cplx *Vs = Qs + UD_STAGES * per;                 // [UD_STAGES][v_in, w_in][TR]
-    cplx *hs = Vs + UD_STAGES * 2 * TR;              // c1 h1 + c2 h2
-    cplx *red = hs + ncols;                          // [UD_WARPS][32] partial sums of Q h
-    cplx *vs = red + UD_WARPS * 32;                  // the tile's v_out
-    double *nsq_s = reinterpret_cast<double *>(vs + TR);
+    const int per = ncols * UD_TR;
+    cplx *Qs = ud_smem;                         // two tiles, [ncols][UD_TR] each
+    cplx *hs = Qs + 2 * per;                    // c1 h1 + c2 h2
+    cplx *red = hs + ncols;                     // [UD_WARPS][UD_TR] partial sums of Q h
+    cplx *vs = red + UD_WARPS * UD_TR;          // the tile's v_out
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int r = lane % TR, grp = lane / TR;
     for (int j = tid; j < ncols; j += blockDim.x) {
         cplx h = cmul(c1, h1[j]);
         if (h2) cfma(h, c2, h2[j]);
         hs[j] = h;
     }
-    const int64_t ntiles = (n + TR - 1) / TR;
-    // one commit group per call, empty past the last tile; rows past n (and
-    // an absent v_in or w_in) are zero-filled: source size 0 from a valid
-    // address
-    auto issue = [&](int64_t tile, int slot) {
-        if (tile < ntiles) {
-            const int64_t row0 = tile * TR;
-            cplx *dst = Qs + slot * per;
-            for (int e = tid; e < per; e += blockDim.x) {
-                const int j = e / TR, rr = e % TR;
-                const int64_t row = row0 + rr;
-                const bool in = row < n;
-                cp_async16(dst + e, Q + (int64_t)j * ld + (in ? row : 0), in ? 16 : 0);
-            }
-            if (tid < 2 * TR) {
-                const cplx *src = tid < TR ? v_in : w_in;
-                const int64_t row = row0 + tid % TR;
-                const bool in = src && row < n;
-                cp_async16(Vs + slot * 2 * TR + tid, in ? src + row : Q, in ? 16 : 0);
-            }
+    const int64_t ntiles = (n + UD_TR - 1) / UD_TR;
+    // rows past n are zero-filled (source size 0), so they add nothing
+    auto issue = [&](int64_t tile, cplx *dst) {
+        const int64_t row0 = tile * UD_TR;
+        for (int e = tid; e < per; e += blockDim.x) {
+            const int j = e >> 5, r = e & 31;
+            const int64_t row = row0 + r;
+            const bool in = row < n;
+            cp_async16(dst + e, Q + (int64_t)j * ld + (in ? row : 0), in ? 16 : 0);
         }
         asm volatile("cp.async.commit_group;\n" ::: "memory");
     };
-    cplx acc[CPL];
+    cplx acc[UD_CPW];
 #pragma unroll
-    for (int c = 0; c < CPL; ++c) acc[c] = mk(0.0, 0.0);
+    for (int c = 0; c < UD_CPW; ++c) acc[c] = mk(0.0, 0.0);
     double nsq = 0.0;
-    const int64_t G = gridDim.x;
-#pragma unroll
-    for (int s = 0; s < UD_STAGES - 1; ++s) issue(blockIdx.x + s * G, s);
-    int slot = 0;
-    for (int64_t tile = blockIdx.x; tile < ntiles; tile += G) {
-        asm volatile("cp.async.wait_group %0;\n" ::"n"(UD_STAGES - 2) : "memory");
-        __syncthreads();                             // this tile landed; the slot used last is free
-        issue(tile + (UD_STAGES - 1) * G, (slot + UD_STAGES - 1) % UD_STAGES);
-        const cplx *Qt = Qs + slot * per;
-        const cplx *Vt = Vs + slot * 2 * TR;
+    int buf = 0;
+    int64_t tile = blockIdx.x;
+    if (tile < ntiles) issue(tile, Qs);
+    for (; tile < ntiles; tile += gridDim.x) {
+        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+        __syncthreads();                        // tile landed; the other buffer is free
+        const int64_t next = tile + gridDim.x;
+        if (next < ntiles) issue(next, Qs + (buf ^ 1) * per);
+        const cplx *Qt = Qs + buf * per;
+        const int64_t row = tile * UD_TR + lane;
+        cplx base = mk(0.0, 0.0);
+        if (warp == 0 && row < n) {
+            if (v_in) base = cmul(a, v_in[row]);
+            if (w_in) cfma(base, b, w_in[row]);
+        }
         cplx p = mk(0.0, 0.0);
 #pragma unroll
-        for (int c = 0; c < CPL; ++c) {
-            const int j = warp + UD_WARPS * (H * c + grp);
-            if (j < ncols) cfma(p, Qt[j * TR + r], hs[j]);
+        for (int c = 0; c < UD_CPW; ++c) {
+            const int j = warp + UD_WARPS * c;
+            if (j < ncols) cfma(p, Qt[j * UD_TR + lane], hs[j]);
         }
-        red[warp * 32 + lane] = p;
+        red[warp * UD_TR + lane] = p;
         __syncthreads();
-        {
-            // P consecutive threads own one row: its partials from warp
-            // part % 16, lane row + TR (part / 16)
-            const int row_l = tid / P, part = tid % P;
-            cplx x = red[(part % UD_WARPS) * 32 + row_l + TR * (part / UD_WARPS)];
-#pragma unroll
-            for (int o = P / 2; o > 0; o >>= 1) {
-                x.x += __shfl_xor_sync(0xffffffffu, x.x, o);
-                x.y += __shfl_xor_sync(0xffffffffu, x.y, o);
-            }
-            if (part == 0) {
-                const int64_t row = tile * TR + row_l;
-                cplx vo = mk(0.0, 0.0);
-                if (row < n) {
-                    cplx base = mk(0.0, 0.0);
-                    if (v_in) base = cmul(a, Vt[row_l]);
-                    if (w_in) cfma(base, b, Vt[TR + row_l]);
-                    vo = csub(base, x);
-                    v_out[row] = vo;
-                    nsq += cabs2(vo);
-                }
-                vs[row_l] = vo;
+        if (warp == 0) {
+            cplx sum = red[lane];
+            for (int w = 1; w < UD_WARPS; ++w) sum = cadd(sum, red[w * UD_TR + lane]);
+            const cplx vo = row < n ? csub(base, sum) : mk(0.0, 0.0);
+            vs[lane] = vo;
+            if (row < n) {
+                v_out[row] = vo;
+                nsq += cabs2(vo);
             }
         }
         __syncthreads();
-        const cplx vo = vs[r];
+        const cplx vo = vs[lane];
 #pragma unroll
-        for (int c = 0; c < CPL; ++c) {
-            const int j = warp + UD_WARPS * (H * c + grp);
-            if (j < ncols) cfmac(acc[c], Qt[j * TR + r], vo);
+        for (int c = 0; c < UD_CPW; ++c) {
+            const int j = warp + UD_WARPS * c;
+            if (j < ncols) cfmac(acc[c], Qt[j * UD_TR + lane], vo);
         }
-        slot = (slot + 1) % UD_STAGES;
+        buf ^= 1;
     }
-    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-    // column sums over the TR lanes that share a column
     cplx *out = partial + (int64_t)blockIdx.x * (ncols + 1);
 #pragma unroll
-    for (int c = 0; c < CPL; ++c) {
-        cplx v = acc[c];
-#pragma unroll
-        for (int o = TR / 2; o > 0; o >>= 1) {
-            v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
-            v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
-        }
-        const int j = warp + UD_WARPS * (H * c + grp);
-        if (r == 0 && j < ncols) out[j] = v;
+    for (int c = 0; c < UD_CPW; ++c) {
+        const int j = warp + UD_WARPS * c;
+        const cplx sum = warp_sum(acc[c]);
+        if (lane == 0 && j < ncols) out[j] = sum;
     }
-    const double wsum = warp_sum(nsq);
-    if (lane == 0) nsq_s[warp] = wsum;
-    __syncthreads();
     __shared__ bool last;
-    if (tid == 0) {
-        double t = 0.0;
-        for (int w = 0; w < UD_WARPS; ++w) t += nsq_s[w];
-        out[ncols] = mk(t, 0.0);
-        nrm_part[blockIdx.x] = t;
-        __threadfence();
-        last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+    if (warp == 0) {
+        const double t = warp_sum(nsq);
+        if (lane == 0) {
+            out[ncols] = mk(t, 0.0);
+            nrm_part[blockIdx.x] = t;
+            __threadfence();
+            last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+        }
     }
     __syncthreads();
     if (!last || warp != 0) return;
@@ -667,33 +620,23 @@ bbjd_status cgs_tail(Scratch &S, int ncols, int64_t ld, const cplx *Q, const cpl
                      const cplx *w_in, cplx *v_out, double *norm_out, const cplx *ref_nsq,
                      const double *ref_nrm, int *flag, cplx *h_re, cudaStream_t st) {
     bbjd_status s;
-    const int tr = ncols + 1 <= S.maxX ? update_dot_rows(ncols) : 0;
-    if (tr) {
+    if (ncols > 0 && update_dot_fits(ncols) && ncols + 1 <= S.maxX) {
         static std::once_flag once;
         static cudaError_t attr = cudaSuccess;
         std::call_once(once, [] {
-            attr = cudaFuncSetAttribute(k_update_dot<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            attr = cudaFuncSetAttribute(k_update_dot, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)UD_SMEM_LIMIT);
-            if (attr == cudaSuccess)
-                attr = cudaFuncSetAttribute(k_update_dot<16>,
-                                            cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            (int)UD_SMEM_LIMIT);
         });
         if (attr != cudaSuccess) {
             set_last_error(attr, "cudaFuncSetAttribute(k_update_dot)", __FILE__, __LINE__);
             return BBJD_ERR_CUDA;
         }
-        const int64_t ntiles = (S.n + tr - 1) / tr;
+        const int64_t ntiles = (S.n + UD_TR - 1) / UD_TR;
         const int G = (int)std::max<int64_t>(1, std::min<int64_t>({(int64_t)num_sms(), ntiles,
                                                                     (int64_t)S.G}));
-        if (tr == 32)
-            k_update_dot<32><<<G, UD_WARPS * 32, update_dot_smem<32>(ncols), st>>>(
-                S.n, ncols, ld, Q, h1, h2, c1, c2, a, v_in, b, w_in, v_out, S.partial, S.nrm_part,
-                S.counter, norm_out, ref_nsq, ref_nrm, flag);
-        else
-            k_update_dot<16><<<G, UD_WARPS * 32, update_dot_smem<16>(ncols), st>>>(
-                S.n, ncols, ld, Q, h1, h2, c1, c2, a, v_in, b, w_in, v_out, S.partial, S.nrm_part,
-                S.counter, norm_out, ref_nsq, ref_nrm, flag);
+        k_update_dot<<<G, UD_WARPS * 32, update_dot_smem(ncols), st>>>(
+            S.n, ncols, ld, Q, h1, h2, c1, c2, a, v_in, b, w_in, v_out, S.partial, S.nrm_part,
+            S.counter, norm_out, ref_nsq, ref_nrm, flag);
         BBJD_LAUNCH_CHECK();
         k_reduce<<<(ncols + 1 + 31) / 32, 256, 0, st>>>(S.partial, G, ncols + 1, h_re, flag);
         BBJD_LAUNCH_CHECK();
