@@ -45,13 +45,15 @@ WORKLOAD_NAME = "bbt_n1000064_k64"
 # Outer iterations per converged eigenpair of the FP64 device engine on this
 # pencil (same algorithm and start vector as the reference), used to turn
 # the reference's measured seconds per outer iteration into eigenpairs/s.
-PAIRS_PER_ITER = 10 / 2000   # measured: 10 pairs in the 2000-iteration cap (FP64, B200)
+PAIRS_PER_ITER = 10 / 2000   # measured: 10 pairs in the 2000-iteration cap (B200)
 # DRAM traffic (read + write bytes) of each kernel class per call, from ncu
 # captures on B200 (profiles/): the fused A,B product per launch, and the
 # ratio of measured DRAM bytes to algorithmic bytes for the CGS classes
-# (all their launches over 250 outer iterations, selected by NVTX range).
+# (all their launches over 150 outer iterations, selected by NVTX range;
+# captured with an earlier tiling of the fused CGS update that moves the
+# same bytes).
 SPMV_TRAFFIC_BYTES = 4.117e9   # profiles/launch_list_bbt_n1000064.md: 317.04 GB / 77 launches
-TRAFFIC_RATIO = {"pencil": 2418.65 / 2422.01, "orth": 1602.48 / 1606.63}   # profiles/class_traffic_bbt_n1000064.md
+TRAFFIC_RATIO = {"pencil": 916.86 / 918.04, "orth": 546.50 / 548.07}   # profiles/launch_list_fused_cgs_bbt_n1000064.md
 
 
 def _env_rank():
