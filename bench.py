@@ -52,8 +52,8 @@ PAIRS_PER_ITER = 10 / 2000   # measured: 10 pairs in the 2000-iteration cap (B20
 # (all their launches over 150 outer iterations, selected by NVTX range;
 # captured with an earlier tiling of the fused CGS update that moves the
 # same bytes).
-SPMV_TRAFFIC_BYTES = 4.117e9   # profiles/launch_list_bbt_n1000064.md: 317.04 GB / 77 launches
-TRAFFIC_RATIO = {"pencil": 916.86 / 918.04, "orth": 546.50 / 548.07}   # profiles/launch_list_fused_cgs_bbt_n1000064.md
+SPMV_TRAFFIC_BYTES = 4.117e9   # launch list, n = 1,000,064: 317.04 GB over 77 launches
+TRAFFIC_RATIO = {"pencil": 916.86 / 918.04, "orth": 546.50 / 548.07}   # GB measured / algorithmic
 
 
 def _env_rank():

@@ -44,7 +44,7 @@ def test_static_matches_allocating_twice(n, k):
     # two calls in a row: the shared scratch keeps the first call's contents
     for _ in range(2):
         got_v, got_n, got_s = _orth(lib.bbjd_dev_orthogonalize_static, Qd, n, k, v)
-        # FP64, same kernels and launch shapes: 1e-12 relative (the kernel tests' bound)
+        # FP64: 1e-12 relative (the kernel tests' bound)
         assert np.linalg.norm(got_v - ref_v) <= 1e-12 * np.linalg.norm(v)
         assert abs(got_n - ref_n) <= 1e-12 * max(1.0, ref_n)
         assert got_s == ref_s
