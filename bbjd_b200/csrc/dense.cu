@@ -556,6 +556,9 @@ bbjd_status Scratch::init(int64_t n_, int max_cols, int nvec) {
     BBJD_CUDA_TRY(cudaMalloc(&scal, sizeof(double) * 64));
     BBJD_CUDA_TRY(cudaMalloc(&flags, sizeof(int) * 16));
     BBJD_CUDA_TRY(cudaMemset(flags, 0, sizeof(int) * 16));
+    // the fused CGS update stages tiles of the basis in up to 226 KB
+    BBJD_CUDA_TRY(cudaFuncSetAttribute(k_update_dot, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)UD_SMEM_LIMIT));
     size_t smem_need = sizeof(cplx) * 2 * (size_t)rpc;
     if (smem_need > 48 * 1024) {
         BBJD_CUDA_TRY(cudaFuncSetAttribute(k_tsdot<1, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_need));
@@ -621,16 +624,7 @@ bbjd_status cgs_tail(Scratch &S, int ncols, int64_t ld, const cplx *Q, const cpl
                      const double *ref_nrm, int *flag, cplx *h_re, cudaStream_t st) {
     bbjd_status s;
     if (ncols > 0 && update_dot_fits(ncols) && ncols + 1 <= S.maxX) {
-        static std::once_flag once;
-        static cudaError_t attr = cudaSuccess;
-        std::call_once(once, [] {
-            attr = cudaFuncSetAttribute(k_update_dot, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)UD_SMEM_LIMIT);
-        });
-        if (attr != cudaSuccess) {
-            set_last_error(attr, "cudaFuncSetAttribute(k_update_dot)", __FILE__, __LINE__);
-            return BBJD_ERR_CUDA;
-        }
+        // the shared-memory limit was raised on this device by Scratch::init
         const int64_t ntiles = (S.n + UD_TR - 1) / UD_TR;
         const int G = (int)std::max<int64_t>(1, std::min<int64_t>({(int64_t)num_sms(), ntiles,
                                                                     (int64_t)S.G}));
