@@ -52,8 +52,10 @@ int main(void) {
     P(bbjd_result, eigenvectors); P(bbjd_result, iters); P(bbjd_result, status);
     P(bbjd_workspace, MA); P(bbjd_workspace, nlock); P(bbjd_workspace, gmres_V);
     P(bbjd_workspace, inner_maxiter); P(bbjd_workspace, swap_nm); P(bbjd_workspace, h_work);
-    P(bbjd_device_ext, evec_layout); P(bbjd_device_ext, seconds_total);
-    P(bbjd_device_ext, kernel_launches);
+    P(bbjd_device_ext, evec_layout); P(bbjd_device_ext, ritz_estimate);
+    P(bbjd_device_ext, seconds_total); P(bbjd_device_ext, kernel_launches);
+    P(bbjd_device_ext, duplicates); P(bbjd_device_ext, ritz_refinements);
+    P(bbjd_device_ext, ritz_fallbacks);
     P(bbjd_device_ext, kernel_ms); P(bbjd_device_ext, kernel_calls);
     return 0;
 }
