@@ -74,7 +74,8 @@ def solve_share(P, sigmas, idx, args):
         res, _ = jdqz_batch([dev] * len(chunk), [sigmas[i] for i in chunk], k=args.k, tol=args.tol,
                             maxiter=args.maxiter, maxsub=args.maxsub, minsub=args.minsub,
                             precision=args.precision, threads=len(chunk),
-                            v0s=[start_vector(P.n, 1 + i) for i in chunk])
+                            v0s=[start_vector(P.n, 1 + i) for i in chunk],
+                            ritz_estimate=args.ritz_estimate)
         for i, (ev, evecs, info) in zip(chunk, res):
             out[i] = (ev, info["residuals"], info["iters"], info["status"],
                       evecs if args.vectors else None)
@@ -97,6 +98,9 @@ def main(argv=None) -> int:
     ap.add_argument("--maxsub", type=int, default=0)
     ap.add_argument("--minsub", type=int, default=0)
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--ritz-estimate", default="auto", choices=["auto", "fp64", "fp32"],
+                    help="projected eigenvalues between restarts: complex64 estimates with "
+                         "an FP64-refined target (auto, fp32) or all in FP64")
     ap.add_argument("--threads", type=int, default=4, help="concurrent solves per GPU")
     ap.add_argument("--vectors", action="store_true", help="also gather the eigenvectors")
     ap.add_argument("--out", default="sweep.npz")
