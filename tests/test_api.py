@@ -29,3 +29,10 @@ def test_device_pencil_arrays_are_size_checked():
     strided = dict(d, Ad=np.repeat(d["Ad"], 2)[::2])
     with pytest.raises(ValueError, match="not contiguous"):
         DevicePencil(arrays=strided, b=8, nblk=4, t=2)
+
+
+def test_ritz_estimate_values_checked():
+    from bbjd_b200 import jdqz_batch, make_pencil
+    P = make_pencil(8, 4, 2, seed=0)
+    with pytest.raises(ValueError, match="ritz_estimate must be one of"):
+        jdqz_batch([P], [3.0], k=1, ritz_estimate="fp16")
