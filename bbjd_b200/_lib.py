@@ -68,12 +68,14 @@ class DeviceExt(C.Structure):
     _fields_ = [
         ("precision", C.c_int), ("record_timing", C.c_int), ("projected", C.c_int),
         ("lock_rule", C.c_int), ("lock_rel", C.c_double), ("stream", C.c_void_p),
-        ("evec_layout", C.c_int), ("ritz_estimate", C.c_int), ("seconds_total", C.c_double),
+        ("evec_layout", C.c_int), ("ritz_estimate", C.c_int), ("host_overlap", C.c_int),
+        ("conv_iters", C.c_void_p), ("seconds_total", C.c_double),
         ("seconds_qz", C.c_double), ("seconds_device", C.c_double),
         ("seconds_restart", C.c_double), ("bytes_device", C.c_double),
         ("kernel_launches", C.c_int64), ("dgks_passes", C.c_int64), ("restarts", C.c_int64),
         ("duplicates", C.c_int64), ("ritz_refinements", C.c_int64),
-        ("ritz_fallbacks", C.c_int64),
+        ("ritz_fallbacks", C.c_int64), ("seconds_qz_exposed", C.c_double),
+        ("guess_hits", C.c_int64), ("guess_misses", C.c_int64),
         ("kernel_ms", C.c_double * 8), ("kernel_bytes", C.c_double * 8),
         ("kernel_calls", C.c_int64 * 8),
     ]

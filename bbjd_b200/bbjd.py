@@ -304,11 +304,12 @@ def jdqz_c(n, nev, sigma, target, matvec_A, matvec_B, precond_solve, tol=1e-10, 
 _PROJECTED = {"auto": 0, "qz": 1, "schur": 2}
 _LOCK = {"robust": 0, "reference": 1}
 _RITZ = {"auto": 0, "fp64": 1, "fp32": 2}
+_OVERLAP = {"auto": 0, "off": 1}
 
 
 def _solve_device(dev: DevicePencil, pc, k, sigma, target, tol, maxiter, maxsub, minsub,
                   inner_maxiter, inner_tol, v0, verbose, timing, projected="auto",
-                  lock="robust", precision="fp64", ritz_estimate="auto"):
+                  lock="robust", precision="fp64", ritz_estimate="auto", host_overlap="auto"):
     lib = _lib.load()
     n = dev.n
     p = _lib.Params()
@@ -336,6 +337,11 @@ def _solve_device(dev: DevicePencil, pc, k, sigma, target, tol, maxiter, maxsub,
     if ritz_estimate not in _RITZ:
         raise ValueError(f"ritz_estimate must be one of {list(_RITZ)}")
     ext.ritz_estimate = _RITZ[ritz_estimate]
+    if host_overlap not in _OVERLAP:
+        raise ValueError(f"host_overlap must be one of {list(_OVERLAP)}")
+    ext.host_overlap = _OVERLAP[host_overlap]
+    conv_iters = np.zeros(int(k), dtype=np.int64)
+    ext.conv_iters = conv_iters.ctypes.data
     ext.evec_layout = 1        # BBJD_EVEC_ROW_MAJOR: the (n, nconv) array comes back ready
     ws = lib.bbjd_workspace_alloc(C.byref(p))
     if not ws:
@@ -357,6 +363,9 @@ def _solve_device(dev: DevicePencil, pc, k, sigma, target, tol, maxiter, maxsub,
         "dgks_passes": int(ext.dgks_passes), "restarts": int(ext.restarts),
         "duplicates": int(ext.duplicates), "ritz_refinements": int(ext.ritz_refinements),
         "ritz_fallbacks": int(ext.ritz_fallbacks),
+        "seconds_qz_exposed": ext.seconds_qz_exposed, "guess_hits": int(ext.guess_hits),
+        "guess_misses": int(ext.guess_misses),
+        "conv_iters": conv_iters[:int(res.nconv)].copy(),
         "kernels": {name: {"ms": ext.kernel_ms[i], "bytes": ext.kernel_bytes[i],
                            "calls": int(ext.kernel_calls[i])}
                     for i, name in enumerate(_lib.KERNEL_CLASSES)},
@@ -386,6 +395,7 @@ def jdqz(
     precision: str = "fp64",
     oracle=None,
     ritz_estimate: str = "auto",
+    host_overlap: str = "auto",
 ):
     """Jacobi-Davidson QZ for ``A x = lambda B x``, the eigenvalues nearest
     ``sigma`` first.  Parameters, defaults, returns and errors are those of
@@ -418,6 +428,14 @@ def jdqz(
     eigenpair by Rayleigh-quotient iteration (the FP64 path takes over when
     that does not converge); 'fp64' computes all of them in FP64.  The
     returned values and the convergence test are FP64 either way.
+    ``host_overlap`` (FP32 estimates only): 'auto' computes the estimates
+    on a second host thread while the device iterates on the target guessed
+    from the previous one (a rejected guess repeats that device work); 'off'
+    computes them first.  Both return the same bits.  ``info['device']``
+    reports ``conv_iters`` (the outer iteration at which each returned pair
+    converged), ``guess_hits`` / ``guess_misses`` and
+    ``seconds_qz_exposed`` (the projected-solve seconds not hidden behind
+    the device).
     """
     if which not in _TARGET_MAP:
         raise ValueError(f"which must be one of {list(_TARGET_MAP.keys())}; got {which!r}")
@@ -447,7 +465,8 @@ def jdqz(
         try:
             ev, evecs, resid, nconv, iters, status, stats = _solve_device(
                 dev, pc, k, sigma, target, tol, maxiter, maxsub, minsub, inner_maxiter,
-                inner_tol, v0, verbose, timing, projected, lock, precision, ritz_estimate)
+                inner_tol, v0, verbose, timing, projected, lock, precision, ritz_estimate,
+                host_overlap)
         finally:
             if own_pc:
                 pc.close()
@@ -473,7 +492,7 @@ def jdqz(
                         inner_tol=inner_tol, preconditioner=pc, v0=v0, verbose=verbose,
                         return_info=return_info, timing=timing, projected=projected,
                         lock=lock, precision=precision, oracle=oracle,
-                        ritz_estimate=ritz_estimate)
+                        ritz_estimate=ritz_estimate, host_overlap=host_overlap)
         if isinstance(preconditioner, (str, SparseLU, DevicePreconditioner)):
             raise ValueError("a device preconditioner needs a block-bordered A, B pencil")
 

@@ -169,8 +169,10 @@ static bbjd_status run_engine(const bbjd_params *p, bbjd_workspace *ws, bbjd_res
     if (p->verbose >= 1 && E.proj_mode == BBJD_PROJ_SCHUR)
         fprintf(stderr, "  projected solve %.3f s: form H %.3f, Hessenberg %.3f, eigenvalues %.3f, "
                 "target vector %.3f, restart Schur form + reorder %.3f (FP32 estimates: %lld "
-                "refinement LUs, %lld FP64 fallbacks)\n", E.qz_seconds, E.qz_split[0],
-                E.qz_split[1], E.qz_split[2], E.qz_split[3], E.qz_split[4], E.rq_lus, E.rq_fallbacks);
+                "refinement LUs, %lld FP64 fallbacks); on the driving thread %.3f s; guesses %lld held, "
+                "%lld rejected\n", E.qz_seconds, E.qz_split[0],
+                E.qz_split[1], E.qz_split[2], E.qz_split[3], E.qz_split[4], E.rq_lus, E.rq_fallbacks,
+                E.qz_exposed, E.spec_hits, E.spec_misses);
     if (s != BBJD_ERR_CUDA && !(cb_failed && *cb_failed)) {
         const bbjd_status f = E.finish_eigenvectors();
         if (f != BBJD_SUCCESS) s = f;
@@ -190,6 +192,9 @@ static bbjd_status run_engine(const bbjd_params *p, bbjd_workspace *ws, bbjd_res
         ext->duplicates = E.duplicates;
         ext->ritz_refinements = E.rq_lus;
         ext->ritz_fallbacks = E.rq_fallbacks;
+        ext->seconds_qz_exposed = E.qz_exposed;
+        ext->guess_hits = E.spec_hits;
+        ext->guess_misses = E.spec_misses;
         double dev = 0.0;
         E.T.flush();
         for (int c = 0; c < KC_N && c < 8; ++c) {

@@ -4,6 +4,10 @@
 
 #include <chrono>
 #include <complex>
+#include <condition_variable>
+#include <functional>
+#include <mutex>
+#include <thread>
 #include <vector>
 
 #include "bbt.cuh"
@@ -55,6 +59,21 @@ struct Timer {
     void end();
     void flush();   // after a stream sync
     void release();
+};
+
+// One host thread beside the thread that drives the device: it computes the
+// complex64 eigenvalue estimates of an outer iteration's projected matrix
+// while the device works on the target guessed for that iteration.
+struct HostWorker {
+    std::thread th;
+    std::mutex m;
+    std::condition_variable cv;
+    std::function<void()> job;
+    bool busy = false, quit = false;
+    void submit(std::function<void()> f);
+    void wait();
+    void stop();
+    ~HostWorker() { stop(); }
 };
 
 struct Engine {
@@ -114,6 +133,22 @@ struct Engine {
     std::vector<float> rwork32;
     long long rq_lus = 0, rq_fallbacks = 0;
     std::vector<int> ipiv;
+    // Target guessed from the previous one (the canonical rule of
+    // pick_target): when the previous iteration's target is known, Rayleigh-
+    // quotient iteration from it gives (spec_w, hx) before the k estimates
+    // exist.  spec_async: the estimates then run on `worker` while the device
+    // works on the guess, and are checked before the iteration commits.
+    bool spec_async = false;
+    bool has_prev = false;            // prev_w is the last committed target's omega
+    zc prev_w;
+    bool spec_ok = false;             // this iteration has a guess (spec_w, hx)
+    zc spec_w;
+    bool est_pending = false;         // estimates running on the worker
+    bool est_ok = false;              // estimates finished and finite
+    double est_seconds = 0;           // worker seconds of the pending estimates
+    HostWorker worker;
+    long long spec_hits = 0, spec_misses = 0;
+    double qz_exposed = 0;            // projected-solve seconds on the driving thread
     double qz_seconds = 0;
     // host seconds of the Schur-form projected solve: forming H, Hessenberg
     // reduction, eigenvalues (QR), target vector, restart Schur form + reorder
@@ -148,9 +183,15 @@ struct Engine {
     void hessenberg_eigvec(int k, zc w, zc *x);
     void dense_eigvec(int k, zc w, zc *x);
     bool eigenvalues32(int k);
+    int form_H(int k);
+    int eig_fp64(int k, int nkeep, bool reorder, int *target_pos);
+    int projected_begin(int k, int nkeep, bool reorder, int *target_pos);
+    int projected_resolve(int k, int *target_pos, bool *changed);
+    int pick_target(int k, int *target_pos, bool *guessed);
     bool rq_refine(int k, zc &w, zc *x);
     bool refine_target(int k, int *target_pos);
     void to_lambda(int i);
+    void lambda_of(zc w, zc &a, zc &b) const;
     void select_and_scan(int k, int nkeep, int *target_pos);
     void ritz_coefficients(int k, int p, zc ta, zc tb, cplx *x);
     bbjd_status sync();

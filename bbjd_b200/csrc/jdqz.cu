@@ -163,6 +163,43 @@ void Timer::release() {
 }
 
 // ---------------------------------------------------------------------------
+void HostWorker::submit(std::function<void()> f) {
+    std::unique_lock<std::mutex> l(m);
+    if (!th.joinable())
+        th = std::thread([this] {
+            std::unique_lock<std::mutex> lk(m);
+            for (;;) {
+                cv.wait(lk, [this] { return quit || (busy && job); });
+                if (quit && !job) return;
+                std::function<void()> j = std::move(job);
+                job = nullptr;
+                lk.unlock();
+                j();
+                lk.lock();
+                busy = false;
+                cv.notify_all();
+            }
+        });
+    job = std::move(f);
+    busy = true;
+    cv.notify_all();
+}
+void HostWorker::wait() {
+    std::unique_lock<std::mutex> l(m);
+    cv.wait(l, [this] { return !busy; });
+}
+void HostWorker::stop() {
+    {
+        std::unique_lock<std::mutex> l(m);
+        cv.wait(l, [this] { return !busy; });
+        quit = true;
+    }
+    cv.notify_all();
+    if (th.joinable()) th.join();
+    quit = false;
+}
+
+// ---------------------------------------------------------------------------
 bbjd_status Engine::init(const bbjd_params *p, bbjd_workspace *w, bbjd_result *r,
                          bbjd_device_ext *e, Operators *o, cudaStream_t stream) {
     P = p;
@@ -231,6 +268,12 @@ bbjd_status Engine::init(const bbjd_params *p, bbjd_workspace *w, bbjd_result *r
     zwork.resize(64 * (size_t)maxsub + 64);
     ritz32 = !ext || ext->ritz_estimate != BBJD_RITZ_FP64;
     rq_lus = rq_fallbacks = 0;
+    // the estimates overlap the device work of a lone solve; the solves of
+    // bbjd_solve_batch already keep every host core busy
+    spec_async = !g_concurrent_solve && !(ext && ext->host_overlap == BBJD_OVERLAP_OFF);
+    has_prev = spec_ok = est_pending = false;
+    spec_hits = spec_misses = 0;
+    qz_exposed = 0;
     if (ritz32) {
         hC32.resize((size_t)maxsub * maxsub);
         w32.resize(maxsub);
@@ -242,6 +285,8 @@ bbjd_status Engine::init(const bbjd_params *p, bbjd_workspace *w, bbjd_result *r
 }
 
 void Engine::release() {
+    worker.stop();
+    est_pending = false;
     T.release();
     S.release();
     cudaFree(ru); cudaFree(zs); cudaFree(Au); cudaFree(Bu);
@@ -482,12 +527,19 @@ void Engine::select_and_scan(int k, int nkeep, int *target_pos) {
 // Returns 1 when C is singular (the caller falls back to QZ), -1 on a LAPACK
 // error, 0 on success.
 int Engine::solve_projected_schur(int k, int nkeep, bool reorder, int *target_pos) {
-    auto t0 = std::chrono::steady_clock::now();
-    ritz_ready = false;
-    const int bk = k, ld = (int)maxsub, one = 1;
+    const int rc = projected_begin(k, nkeep, reorder, target_pos);
+    if (rc || !est_pending) return rc;
+    bool changed = false;
+    return projected_resolve(k, target_pos, &changed);
+}
+
+// H = C^-1 MB into ws->SA (ld maxsub), and its copy hH (the base of the next
+// iteration's O(k^2) update).  1: C singular; -1: LAPACK error; 0: done.
+int Engine::form_H(int k) {
+    const int bk = k, ld = (int)maxsub;
     int info = 0;
     zc *MA = ws->MA, *MB = ws->MB;
-    zc *T = ws->SA, *Q = ws->ZB;
+    zc *T = ws->SA;
     double c_all = 0.0, c_low = 0.0;
     for (int j = 0; j < k; ++j)
         for (int i = 0; i < k; ++i) {
@@ -558,28 +610,162 @@ int Engine::solve_projected_schur(int k, int nkeep, bool reorder, int *target_po
     // the Schur form below): the base of the next iteration's update
     for (int j = 0; j < k; ++j) memcpy(&hH[(size_t)j * maxsub], T + (size_t)j * maxsub, sizeof(zc) * k);
     hH_k = k;
-    auto t1 = std::chrono::steady_clock::now();
-    qz_split[0] += std::chrono::duration<double>(t1 - t0).count();
-    const int lw = (int)zwork.size();
-    const MklLapack &mkl = mkl_lapack();
-    if (!reorder && ritz32) {
-        // Between restarts the eigenvalues only rank the candidates: FP32
-        // estimates, the winner refined to an FP64 eigenpair of H.
-        const bool ok = eigenvalues32(k);
-        auto t3 = std::chrono::steady_clock::now();
-        if (ok)
-            for (int i = 0; i < k; ++i) to_lambda(i);
-        if (ok && refine_target(k, target_pos)) {
+    return 0;
+}
+
+static double secs_since(std::chrono::steady_clock::time_point t) {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t).count();
+}
+
+// First half of the harmonic Schur-form projected solve of one outer
+// iteration: H, then the target.  Between restarts with FP32 estimates
+// (ritz32) the target follows the canonical rule of pick_target; when the
+// previous target is known its Rayleigh-quotient refinement is computed
+// first (the guess), and with spec_async the k estimates that confirm or
+// reject it are started on the worker thread: est_pending is then set,
+// *target_pos is -1, and the caller works on the guess (spec_w, hx) until
+// projected_resolve.  Restarts and the FP64 form take eig_fp64.
+int Engine::projected_begin(int k, int nkeep, bool reorder, int *target_pos) {
+    const auto t0 = std::chrono::steady_clock::now();
+    ritz_ready = false;
+    est_pending = false;
+    spec_ok = false;
+    int rc = form_H(k);
+    const double th = secs_since(t0);
+    qz_split[0] += th;
+    if (rc) {
+        qz_seconds += th;
+        qz_exposed += th;
+        return rc;
+    }
+    if (reorder || !ritz32) {
+        const auto t1 = std::chrono::steady_clock::now();
+        rc = eig_fp64(k, nkeep, reorder, target_pos);
+        qz_seconds += th + secs_since(t1);
+        qz_exposed += th + secs_since(t1);
+        return rc;
+    }
+    const auto t1 = std::chrono::steady_clock::now();
+    if (has_prev) {
+        zc w = prev_w, a, b;
+        if (rq_refine(k, w, hx.data())) {
+            lambda_of(w, a, b);
+            if (std::abs(b) >= 1e-300 && !is_locked(a / b)) {
+                spec_ok = true;
+                spec_w = w;
+            }
+        }
+    }
+    const double tr = secs_since(t1);
+    qz_split[3] += tr;
+    if (spec_ok && spec_async) {
+        est_pending = true;
+        ritz_ready = true;
+        schur_step = true;
+        *target_pos = -1;
+        worker.submit([this, k] {
+            const auto a = std::chrono::steady_clock::now();
+            est_ok = eigenvalues32(k);
+            est_seconds = secs_since(a);
+        });
+        qz_seconds += th + tr;
+        qz_exposed += th + tr;
+        return 0;
+    }
+    const auto t2 = std::chrono::steady_clock::now();
+    est_ok = eigenvalues32(k);
+    const double te = secs_since(t2);
+    qz_split[2] += te;
+    const auto t3 = std::chrono::steady_clock::now();
+    bool guessed = false;
+    rc = pick_target(k, target_pos, &guessed);
+    const double tp = secs_since(t3);
+    qz_split[3] += tp;
+    qz_seconds += th + tr + te + tp;
+    qz_exposed += th + tr + te + tp;
+    return rc;
+}
+
+// Waits for the estimates started by projected_begin and applies the
+// canonical rule; *changed: the target differs from the guess the caller
+// worked on (its device work is to be repeated with *target_pos).
+int Engine::projected_resolve(int k, int *target_pos, bool *changed) {
+    const auto t0 = std::chrono::steady_clock::now();
+    worker.wait();
+    est_pending = false;
+    qz_split[2] += est_seconds;
+    qz_seconds += est_seconds;
+    const auto t1 = std::chrono::steady_clock::now();
+    bool guessed = false;
+    const int rc = pick_target(k, target_pos, &guessed);
+    qz_split[3] += secs_since(t1);
+    qz_seconds += secs_since(t1);
+    qz_exposed += secs_since(t0);
+    *changed = !guessed;
+    return rc;
+}
+
+// The canonical target rule between restarts (FP32 estimates in omega, valid
+// when est_ok; the guess in spec_w / hx when spec_ok).  The estimates rank
+// the candidates (select_and_scan's order, locked values skipped).  If the
+// winner's estimate is the one nearest the guess and lies within 1e-4
+// |spec_w| of it, the target is the guess: the eigenpair Rayleigh-quotient
+// iteration reached from the previous target, refined to FP64 accuracy.
+// Otherwise the winner is refined from its estimate (refine_target), and if
+// that fails, or the estimates did, the FP64 eigenvalues decide (eig_fp64).
+// Whether the estimates ran beside the device or before it, the same target
+// results, so overlapping them changes no result.
+int Engine::pick_target(int k, int *target_pos, bool *guessed) {
+    *guessed = false;
+    if (est_ok) {
+        for (int i = 0; i < k; ++i) to_lambda(i);
+        if (spec_ok) {
+            int widx = -1, near = -1;
+            double best = DBL_MAX, dmin = DBL_MAX;
+            for (int i = 0; i < k; ++i) {
+                const double d = std::abs(omega[i] - spec_w);
+                if (d < dmin) { dmin = d; near = i; }
+                if (std::abs(beta[i]) < 1e-300) continue;
+                const zc lam = alpha[i] / beta[i];
+                if (is_locked(lam)) continue;
+                const double v = target_value(lam, sigma, target);
+                if (v < best) { best = v; widx = i; }
+            }
+            if (widx >= 0 && widx == near && dmin <= 1e-4 * std::abs(spec_w)) {
+                omega[widx] = spec_w;
+                to_lambda(widx);
+                *target_pos = widx;
+                ritz_ready = true;
+                schur_step = true;
+                *guessed = true;
+                spec_hits++;
+                return 0;
+            }
+            spec_misses++;
+        }
+        if (refine_target(k, target_pos)) {
             ritz_ready = true;
             schur_step = true;
-            auto t4 = std::chrono::steady_clock::now();
-            qz_split[2] += std::chrono::duration<double>(t3 - t1).count();
-            qz_split[3] += std::chrono::duration<double>(t4 - t3).count();
-            qz_seconds += std::chrono::duration<double>(t4 - t0).count();
             return 0;
         }
-        rq_fallbacks++;                  // the FP64 path below; T (= H) is intact
+    } else if (spec_ok) {
+        spec_misses++;
     }
+    rq_fallbacks++;
+    return eig_fp64(k, 0, false, target_pos);
+}
+
+// The FP64 projected eigenvalues (H in ws->SA as form_H left it): between
+// restarts ZGEEV (MKL) or ZGEHRD + ZHSEQR('E') and the target's eigenvector
+// by inverse iteration; at a restart the Schur form ZHSEQR('S','V') and the
+// ZTRSEN reorder that brings the kept values to the leading block.
+int Engine::eig_fp64(int k, int nkeep, bool reorder, int *target_pos) {
+    const auto t1 = std::chrono::steady_clock::now();
+    const int bk = k, ld = (int)maxsub, one = 1;
+    int info = 0;
+    zc *T = ws->SA, *Q = ws->ZB;
+    const int lw = (int)zwork.size();
+    const MklLapack &mkl = mkl_lapack();
     if (!reorder && mkl.zgeev && !g_concurrent_solve) {
         // Between restarts only the eigenvalues and the target's eigenvector
         // are used: eigenvalues by ZGEEV on a copy of H (no vectors), the
@@ -600,10 +786,8 @@ int Engine::solve_projected_schur(int k, int nkeep, bool reorder, int *target_po
             dense_eigvec(k, omega[*target_pos], hx.data());
             ritz_ready = true;
             schur_step = true;
-            auto t4 = std::chrono::steady_clock::now();
             qz_split[2] += std::chrono::duration<double>(t3 - t1).count();
-            qz_split[3] += std::chrono::duration<double>(t4 - t3).count();
-            qz_seconds += std::chrono::duration<double>(t4 - t0).count();
+            qz_split[3] += secs_since(t3);
             return 0;
         }
         // ZGEEV did not converge: the OpenBLAS path below
@@ -629,10 +813,8 @@ int Engine::solve_projected_schur(int k, int nkeep, bool reorder, int *target_po
         hessenberg_eigvec(k, omega[*target_pos], hx.data());
         ritz_ready = true;
         schur_step = true;
-        auto t4 = std::chrono::steady_clock::now();
         qz_split[2] += std::chrono::duration<double>(t3 - t2).count();
-        qz_split[3] += std::chrono::duration<double>(t4 - t3).count();
-        qz_seconds += std::chrono::duration<double>(t4 - t0).count();
+        qz_split[3] += secs_since(t3);
         return 0;
     }
     for (int j = 0; j < k; ++j) memcpy(Q + (size_t)j * maxsub, T + (size_t)j * maxsub, sizeof(zc) * k);
@@ -657,9 +839,7 @@ int Engine::solve_projected_schur(int k, int nkeep, bool reorder, int *target_po
     }
     select_and_scan(k, 0, target_pos);
     schur_step = true;
-    const auto t5 = std::chrono::steady_clock::now();
-    qz_split[4] += std::chrono::duration<double>(t5 - t2).count();
-    qz_seconds += std::chrono::duration<double>(t5 - t0).count();
+    qz_split[4] += secs_since(t2);
     return 0;
 }
 
@@ -742,18 +922,18 @@ void Engine::dense_eigvec(int k, zc w, zc *x) {
     back_solve(x);
 }
 
-// lambda = (1 / omega - mu0) / nu0 of position i into alpha[i] / beta[i]
-// (beta = 0: omega = 0, an infinite lambda).
-void Engine::to_lambda(int i) {
-    const zc w = omega[i];
+// lambda = (1 / omega - mu0) / nu0 as a / b, of position i into alpha[i] /
+// beta[i] (b = 0: omega = 0, an infinite lambda).
+void Engine::lambda_of(zc w, zc &a, zc &b) const {
     if (std::abs(w) < 1e-300 * std::abs(nu0)) {
-        alpha[i] = 1.0;
-        beta[i] = 0.0;
+        a = 1.0;
+        b = 0.0;
         return;
     }
-    alpha[i] = (1.0 / w - mu0) / nu0;
-    beta[i] = 1.0;
+    a = (1.0 / w - mu0) / nu0;
+    b = 1.0;
 }
+void Engine::to_lambda(int i) { lambda_of(omega[i], alpha[i], beta[i]); }
 
 // FP32 estimates of the k eigenvalues of H (= ws->SA, ld maxsub) into
 // omega.  H is scaled by a power of two (exact) so that its largest
@@ -1166,15 +1346,39 @@ bbjd_status Engine::run() {
             if (nkeep < 1) nkeep = 1;
             int rc = 1;
             if (proj_mode == BBJD_PROJ_SCHUR)
-                rc = solve_projected_schur((int)k, (int)nkeep, k >= maxsub, &tpos);
+                rc = projected_begin((int)k, (int)nkeep, k >= maxsub, &tpos);
             if (rc > 0) rc = solve_projected((int)k, (int)locked, (int)nkeep, &tpos);
             if (rc) {
                 res->status = BBJD_ERR_LAPACK;
                 return res->status;
             }
         }
-        // Ritz pair at the target position (jd_core.c:851-872)
-        const zc ta = alpha[tpos], tb = beta[tpos];
+        // Target pair (jd_core.c:851-872).  With est_pending the target is the
+        // guess of projected_begin while the estimates that decide it run on
+        // the worker thread; `settle` waits for them before the first step that
+        // cannot be undone (a lock, a random vector drawn, the iteration's
+        // commit) and, if they pick another target, the device work restarts
+        // from the Ritz vector with it (its writes so far went to column k of
+        // V, AV, BV, W and MA, MB, which the repeat overwrites).
+        zc ta, tb;
+        if (est_pending)
+            lambda_of(spec_w, ta, tb);
+        else
+            ta = alpha[tpos], tb = beta[tpos];
+        auto settle = [&](bool *redo) -> bbjd_status {
+            *redo = false;
+            if (!est_pending) return BBJD_SUCCESS;
+            bool changed = false;
+            if (projected_resolve((int)k, &tpos, &changed)) return res->status = BBJD_ERR_LAPACK;
+            if (changed) {
+                ta = alpha[tpos];
+                tb = beta[tpos];
+                *redo = true;
+            }
+            return BBJD_SUCCESS;
+        };
+        bool redo_it = false;
+    redo:
         ritz_coefficients((int)k, tpos, ta, tb, pin);
         BBJD_CUDA_TRY(cudaMemcpyAsync(xdev, pin, sizeof(cplx) * k, cudaMemcpyHostToDevice, st));
         // u = V x, ||u||, u /= ||u||  (jd_core.c:871-877)
@@ -1206,6 +1410,9 @@ bbjd_status Engine::run() {
                     (long long)iter, (long long)k, (long long)locked, lam.real(), lam.imag(), rel);
         }
         if (rel < tol) {                                            // jd_core.c:905-932
+            if ((s = settle(&redo_it))) return s;
+            if (redo_it) goto redo;
+            has_prev = false;             // the next target is another pair
             const zc lam = std::abs(tb) > 1e-300 ? ta / tb : ta;
             if (lock_rule == BBJD_LOCK_ROBUST && ws->nlock > 0 && !locks.empty()) {
                 // is u (to 1e-8) inside the span of the locked Schur vectors,
@@ -1244,6 +1451,7 @@ bbjd_status Engine::run() {
                 BBJD_CUDA_TRY(cudaMemcpyAsync(res->eigenvectors + (size_t)res->nconv * n, u,
                                               sizeof(cplx) * n, cudaMemcpyDeviceToHost, st));
             res->residuals[res->nconv] = rel;
+            if (ext && ext->conv_iters) ext->conv_iters[res->nconv] = iter;
             res->nconv++;
             if (P->verbose >= 1)
                 fprintf(stderr, "  *** converged #%lld: (%+.10e, %+.10e)  res %.3e  iter %lld\n",
@@ -1344,6 +1552,8 @@ bbjd_status Engine::run() {
         if ((s = sync())) return s;
         if (pin_i[FL_T]) { dgks++; second_pass_bytes(KC_ORTH, (int)k); }
         if (pin_d[SC_VNORM] < 1e-14) {
+            if ((s = settle(&redo_it))) return s;
+            if (redo_it) goto redo;
             std::vector<zc> rv(n);
             for (int64_t i = 0; i < n; ++i) {
                 const double re = (double)rand() / RAND_MAX - 0.5;
@@ -1405,10 +1615,15 @@ bbjd_status Engine::run() {
         bytes_dev += 16.0 * n * (2.0 * (k + 1) + 1.0);
         BBJD_CUDA_TRY(cudaMemcpyAsync(pin, S.red, sizeof(cplx) * 2 * (k + 1), cudaMemcpyDeviceToHost, st));
         if ((s = sync())) return s;
+        if ((s = settle(&redo_it))) return s;
+        if (redo_it) goto redo;
         for (int64_t i = 0; i <= k; ++i) {
             ws->MA[k + (size_t)i * maxsub] = std::conj(Z(pin[i]));
             ws->MB[k + (size_t)i * maxsub] = std::conj(Z(pin[k + 1 + i]));
         }
+        // the committed target starts the next iteration's guess
+        has_prev = proj_mode == BBJD_PROJ_SCHUR && schur_step && ritz32;
+        if (has_prev) prev_w = omega[tpos];
         ws->kdim = k + 1;
         res->iters = iter + 1;
     }

@@ -70,6 +70,17 @@ enum { BBJD_EVEC_COLUMN_MAJOR = 0, BBJD_EVEC_ROW_MAJOR = 1 };
  * residuals and the convergence test are FP64 either way.  AUTO = FP32. */
 enum { BBJD_RITZ_AUTO = 0, BBJD_RITZ_FP64 = 1, BBJD_RITZ_FP32 = 2 };
 
+/* Host/device overlap of the FP32-estimate target rule (bbjd_device_ext.
+ * host_overlap).  Between restarts the target is, by rule, the eigenpair that
+ * Rayleigh-quotient iteration reaches from the previous target when the k
+ * complex64 estimates rank it first, else the estimates' winner refined in
+ * FP64.  AUTO: a lone solve computes that guess first, starts the device
+ * iteration on it, and checks it against the estimates computed meanwhile
+ * on a second host thread; a rejected guess repeats the iteration's device
+ * work with the right target.  OFF: the same rule, serially.  Both give the
+ * same results bit for bit.  The solves of bbjd_solve_batch run serially. */
+enum { BBJD_OVERLAP_AUTO = 0, BBJD_OVERLAP_OFF = 1 };
+
 enum { BBJD_PC_NONE = 0, BBJD_PC_BBT_LU = 1, BBJD_PC_BLOCK_JACOBI = 2 };
 
 /* Copy a BBT pencil to the current device.  from_host = 1: pointers are host
@@ -121,6 +132,11 @@ typedef struct {
                                    device at the end of the solve (saves the
                                    host an O(n nconv) strided copy)          */
     int     ritz_estimate;      /* BBJD_RITZ_AUTO (default), _FP64 or _FP32     */
+    int     host_overlap;       /* BBJD_OVERLAP_AUTO (default) or _OFF          */
+    int64_t *conv_iters;        /* optional (NULL): nev entries, filled with the
+                                   outer iteration at which each returned pair
+                                   converged (0-based, as the reference's
+                                   verbose log numbers them)                 */
     /* out */
     double  seconds_total;      /* wall time of the solve                       */
     double  seconds_qz;         /* host projected QZ + reorder                  */
@@ -134,6 +150,11 @@ typedef struct {
     int64_t ritz_refinements;   /* FP64 LU factorisations of the FP32 target
                                    refinement (BBJD_RITZ_FP32)                */
     int64_t ritz_fallbacks;     /* FP32 estimates replaced by the FP64 path    */
+    double  seconds_qz_exposed; /* of seconds_qz, the part the thread driving
+                                   the device spent (not hidden behind it)     */
+    int64_t guess_hits;         /* iterations whose guessed target held         */
+    int64_t guess_misses;       /* guesses rejected (device work repeated when
+                                   host_overlap is AUTO)                      */
     double  kernel_ms[8];       /* per kernel class: spmv, orth, pencil, ritz,
                                    precond, restart, small, gmres (if timed)    */
     double  kernel_bytes[8];

@@ -55,7 +55,9 @@ int main(void) {
     P(bbjd_device_ext, evec_layout); P(bbjd_device_ext, ritz_estimate);
     P(bbjd_device_ext, seconds_total); P(bbjd_device_ext, kernel_launches);
     P(bbjd_device_ext, duplicates); P(bbjd_device_ext, ritz_refinements);
-    P(bbjd_device_ext, ritz_fallbacks);
+    P(bbjd_device_ext, ritz_fallbacks); P(bbjd_device_ext, host_overlap);
+    P(bbjd_device_ext, conv_iters); P(bbjd_device_ext, seconds_qz_exposed);
+    P(bbjd_device_ext, guess_hits); P(bbjd_device_ext, guess_misses);
     P(bbjd_device_ext, kernel_ms); P(bbjd_device_ext, kernel_calls);
     return 0;
 }

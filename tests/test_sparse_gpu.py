@@ -10,7 +10,7 @@ import scipy.sparse as sp
 from scipy.sparse.linalg import splu
 
 from bbjd_b200 import SparseLU, jdqz, make_pencil, start_vector
-from tests.parity import EIG_ATOL, assert_no_duplicates, match_set
+from tests.parity import assert_eigs_match, assert_no_duplicates, nearest
 
 pytestmark = pytest.mark.gpu
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
@@ -53,8 +53,9 @@ def test_readme_pattern_with_sparse_lu(name):
     for lam, x in zip(ev, evecs.T):
         r = A @ x - lam * (B @ x)
         assert np.linalg.norm(r) / ((nA + abs(lam) * nB) * np.linalg.norm(x)) < 1e-10
-    assert match_set(ev, g["eigenvalues"]).max() < EIG_ATOL
-    assert match_set(g["eigenvalues"], ev).max() < EIG_ATOL
+    assert_eigs_match(P, ev, evecs, g["arpack"])
+    assert_eigs_match(P, ev, evecs, g["eigenvalues"], ref_resid=g["unscaled_residuals"])
+    assert sorted(nearest(ev, g["eigenvalues"])) == list(range(int(g["k"])))
     assert_no_duplicates(ev)
     lu.close()
 

@@ -9,7 +9,7 @@ from scipy.sparse.linalg import splu
 
 from bbjd_b200 import jdqz, make_pencil, start_vector
 from oracle import jdqz_np
-from tests.parity import EIG_ATOL, assert_no_duplicates, match_set
+from tests.parity import assert_eigs_match, assert_no_duplicates, match_set, nearest
 
 pytestmark = pytest.mark.gpu
 
@@ -54,8 +54,11 @@ def test_device_targets_match_oracle(which):
                        v0=v0, **kw)
     assert info["nconv"] == ref["nconv"] == 2
     _residuals_ok(A, B, ev, evecs)
-    assert match_set(ev, ref["eigenvalues"]).max() < EIG_ATOL
-    assert match_set(ref["eigenvalues"], ev).max() < EIG_ATOL
+    # each value within its conditioning-aware bound of the exact (dense)
+    # eigenvalue, and the same two the oracle returns
+    lam_arr = np.asarray(lam)
+    assert_eigs_match(P, ev, evecs, lam_arr)
+    assert sorted(nearest(ev, lam_arr)) == sorted(nearest(ref["eigenvalues"], lam_arr))
     assert_no_duplicates(ev)
     # the 2 found lie among the 6 best of the dense spectrum
     assert match_set(ev, best[:6]).max() < 1e-6
@@ -74,8 +77,11 @@ def test_tau_free_pencil_with_identity_b_runs_on_device():
     ev, evecs, info = jdqz(A, None, preconditioner="exact", **kw)
     assert "device" in info and info["nconv"] == 4
     I = sp.eye(P.n, format="csr", dtype=np.complex128)
-    ev_cb, _, info_cb = jdqz(A, None, preconditioner=splu((A - sigma * I).tocsc()), **kw)
+    ev_cb, x_cb, info_cb = jdqz(A, None, preconditioner=splu((A - sigma * I).tocsc()), **kw)
     assert "device" not in info_cb and info_cb["nconv"] == 4
     _residuals_ok(A, I, ev, evecs)
-    assert match_set(ev, ev_cb).max() < EIG_ATOL
-    assert match_set(ev_cb, ev).max() < EIG_ATOL
+    Pi = make_pencil(16, 40, 0, seed=6)
+    Pi.Bd[:] = np.eye(16)
+    r_cb = [np.linalg.norm(A @ x - l * x) / np.linalg.norm(x) for l, x in zip(ev_cb, x_cb.T)]
+    assert_eigs_match(Pi, ev, evecs, ev_cb, ref_resid=r_cb)
+    assert sorted(nearest(ev, ev_cb)) == [0, 1, 2, 3]
