@@ -695,10 +695,10 @@ static size_t inv_smem() { return sizeof(cplx) * BS * Blk<BS>::LDA; }
 
 template <int BS>
 static bbjd_status set_attrs() {
-    BBJD_CUDA_TRY(cudaFuncSetAttribute(k_bcr_odd<BS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)odd_smem<BS>()));
-    BBJD_CUDA_TRY(cudaFuncSetAttribute(k_bcr_even<BS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)even_smem<BS>()));
-    BBJD_CUDA_TRY(cudaFuncSetAttribute(k_invert_blocks<BS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)inv_smem<BS>()));
-    return BBJD_SUCCESS;
+    bbjd_status s;
+    if ((s = raise_smem_limit((const void *)k_bcr_odd<BS>, odd_smem<BS>()))) return s;
+    if ((s = raise_smem_limit((const void *)k_bcr_even<BS>, even_smem<BS>()))) return s;
+    return raise_smem_limit((const void *)k_invert_blocks<BS>, inv_smem<BS>());
 }
 
 // Levels with at most this many blocks to process run one CTA per block.
@@ -1080,17 +1080,10 @@ extern "C" bbjd_status bbjd_precond_create(const bbjd_bbt_matrix *m, bbjd_zomple
     cudaStream_t st = nullptr;
     bbjd_status s = BBJD_SUCCESS;
     if (cudaMalloc(&pc->err, sizeof(int)) != cudaSuccess) s = BBJD_ERR_ALLOC;
-    static std::mutex attr_mu;
-    static bool attrs = false;
-    if (s == BBJD_SUCCESS) {
-        std::lock_guard<std::mutex> lock(attr_mu);
-        if (!attrs) {
-            s = set_attrs<8>();
-            if (s == BBJD_SUCCESS) s = set_attrs<16>();
-            if (s == BBJD_SUCCESS) s = set_attrs<32>();
-            attrs = (s == BBJD_SUCCESS);
-        }
-    }
+    // per device (raise_smem_limit keeps the largest value set on each)
+    if (s == BBJD_SUCCESS) s = set_attrs<8>();
+    if (s == BBJD_SUCCESS) s = set_attrs<16>();
+    if (s == BBJD_SUCCESS) s = set_attrs<32>();
     if (s == BBJD_SUCCESS) {
         pc->G = (int)std::max<int64_t>(1, std::min<int64_t>(4 * num_sms(), (m->nb + 255) / 256));
         if (cudaMalloc(&pc->tau_part, sizeof(cplx) * (size_t)pc->G * 2 * std::max(1, m->t)) != cudaSuccess ||

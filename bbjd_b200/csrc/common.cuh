@@ -75,6 +75,7 @@ extern std::atomic<long long> g_launches;
 inline void count_launch(int n = 1) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
 int num_sms();
+bbjd_status raise_smem_limit(const void *func, size_t bytes);
 
 }  // namespace bbjd
 

@@ -15,6 +15,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <map>
 #include <mutex>
 
 namespace bbjd {
@@ -521,16 +522,36 @@ __global__ void __launch_bounds__(256) k_gram(int64_t n, int keep, const cplx *_
 
 std::atomic<long long> g_launches{0};
 
+// SM count of the current device (cached per device).
 int num_sms() {
-    static std::once_flag once;
-    static int sms = 0;
-    std::call_once(once, [] {
-        int dev = 0, v = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
-        sms = v > 0 ? v : 148;
-    });
-    return sms;
+    static std::mutex mu;
+    static std::map<int, int> sms;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> g(mu);
+    auto it = sms.find(dev);
+    if (it != sms.end()) return it->second;
+    int v = 0;
+    cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+    return sms[dev] = v > 0 ? v : 148;
+}
+
+// A kernel's dynamic shared-memory limit is a per-device, per-process
+// setting: raise it on the current device to at least `bytes`, never lower
+// it (a concurrent solve on the same device may have raised it further for
+// its own launches).
+bbjd_status raise_smem_limit(const void *func, size_t bytes) {
+    if (bytes <= 48 * 1024) return BBJD_SUCCESS;
+    static std::mutex mu;
+    static std::map<std::pair<int, const void *>, size_t> done;
+    int dev = 0;
+    BBJD_CUDA_TRY(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> g(mu);
+    size_t &cur = done[{dev, func}];
+    if (cur >= bytes) return BBJD_SUCCESS;
+    BBJD_CUDA_TRY(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    cur = bytes;
+    return BBJD_SUCCESS;
 }
 
 static thread_local char g_errbuf[512];
@@ -557,14 +578,12 @@ bbjd_status Scratch::init(int64_t n_, int max_cols, int nvec) {
     BBJD_CUDA_TRY(cudaMalloc(&flags, sizeof(int) * 16));
     BBJD_CUDA_TRY(cudaMemset(flags, 0, sizeof(int) * 16));
     // the fused CGS update stages tiles of the basis in up to 226 KB
-    BBJD_CUDA_TRY(cudaFuncSetAttribute(k_update_dot, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)UD_SMEM_LIMIT));
-    size_t smem_need = sizeof(cplx) * 2 * (size_t)rpc;
-    if (smem_need > 48 * 1024) {
-        BBJD_CUDA_TRY(cudaFuncSetAttribute(k_tsdot<1, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_need));
-        BBJD_CUDA_TRY(cudaFuncSetAttribute(k_tsdot<2, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_need));
-        BBJD_CUDA_TRY(cudaFuncSetAttribute(k_tsdot<1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_need));
-    }
+    bbjd_status s;
+    if ((s = raise_smem_limit((const void *)k_update_dot, UD_SMEM_LIMIT))) return s;
+    const size_t smem_need = sizeof(cplx) * 2 * (size_t)rpc;
+    if ((s = raise_smem_limit((const void *)k_tsdot<1, 2>, smem_need))) return s;
+    if ((s = raise_smem_limit((const void *)k_tsdot<2, 1>, smem_need))) return s;
+    if ((s = raise_smem_limit((const void *)k_tsdot<1, 1>, smem_need))) return s;
     return BBJD_SUCCESS;
 }
 
@@ -594,11 +613,7 @@ bbjd_status tsdot(Scratch &S, int NM, int NV, int ncols, int64_t ld, const cplx 
     return BBJD_SUCCESS;
 }
 
-bbjd_status tsdot_allow_smem(size_t bytes) {
-    if (bytes <= 48 * 1024) return BBJD_SUCCESS;
-    BBJD_CUDA_TRY(cudaFuncSetAttribute(k_tsdot<1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
-    return BBJD_SUCCESS;
-}
+bbjd_status tsdot_allow_smem(size_t bytes) { return raise_smem_limit((const void *)k_tsdot<1, 1>, bytes); }
 
 bbjd_status reduce_partials(const cplx *partial, int G, int X, cplx *out, cudaStream_t st) {
     k_reduce<<<(X + 31) / 32, 256, 0, st>>>(partial, G, X, out, nullptr);
@@ -749,13 +764,9 @@ bbjd_status tsdot32(Scratch &S, int ncols, int64_t ld, const float2 *Q, const cp
                     cudaStream_t st) {
     const int X = ncols + 1;
     if (X > S.maxX) return BBJD_ERR_INVALID;
-    static bool attr = false;
     const size_t smem = sizeof(cplx) * (size_t)S.rpc;
-    if (!attr && smem > 48 * 1024) {
-        BBJD_CUDA_TRY(cudaFuncSetAttribute(k_tsdot<1, 1, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           227 * 1024));
-        attr = true;
-    }
+    bbjd_status s = raise_smem_limit((const void *)k_tsdot<1, 1, float2>, smem);
+    if (s) return s;
     k_tsdot<1, 1, float2><<<S.G, 256, smem, st>>>(S.n, ncols, ld, Q, Q, v, nullptr, S.rpc, S.partial, nullptr);
     BBJD_LAUNCH_CHECK();
     return reduce_partials(S.partial, S.G, X, out, st);

@@ -134,13 +134,14 @@ struct Engine {
     long long rq_lus = 0, rq_fallbacks = 0;
     std::vector<int> ipiv;
     // Target guessed from the previous one (the canonical rule of
-    // pick_target): when the previous iteration's target is known, Rayleigh-
-    // quotient iteration from it gives (spec_w, hx) before the k estimates
-    // exist.  spec_async: the estimates then run on `worker` while the device
+    // pick_target): when the previous iteration's target vector, extended
+    // by a zero, is nearly an eigenvector of the new H, Rayleigh-quotient
+    // iteration from it gives (spec_w, hx) before the k estimates exist.  spec_async: the estimates then run on `worker` while the device
     // works on the guess, and are checked before the iteration commits.
     bool spec_async = false;
-    bool has_prev = false;            // prev_w is the last committed target's omega
-    zc prev_w;
+    bool has_prev = false;            // prev_x: the last committed target's eigenvector of H
+    std::vector<zc> prev_x;           // (k - 1 entries; its residual was prev_rel)
+    double prev_rel = 0;
     bool spec_ok = false;             // this iteration has a guess (spec_w, hx)
     zc spec_w;
     bool est_pending = false;         // estimates running on the worker
@@ -181,14 +182,14 @@ struct Engine {
     int solve_projected(int k, int locked, int nkeep, int *target_pos);
     int solve_projected_schur(int k, int nkeep, bool reorder, int *target_pos);
     void hessenberg_eigvec(int k, zc w, zc *x);
-    void dense_eigvec(int k, zc w, zc *x);
+    void dense_eigvec(int k, zc w, zc *x, const zc *x0 = nullptr);
     bool eigenvalues32(int k);
     int form_H(int k);
     int eig_fp64(int k, int nkeep, bool reorder, int *target_pos);
     int projected_begin(int k, int nkeep, bool reorder, int *target_pos);
     int projected_resolve(int k, int *target_pos, bool *changed);
     int pick_target(int k, int *target_pos, bool *guessed);
-    bool rq_refine(int k, zc &w, zc *x);
+    bool rq_refine(int k, zc &w, zc *x, const zc *x0 = nullptr, int max_lu = 5);
     bool refine_target(int k, int *target_pos);
     void to_lambda(int i);
     void lambda_of(zc w, zc &a, zc &b) const;

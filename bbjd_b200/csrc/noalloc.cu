@@ -7,8 +7,12 @@
 // them: its reduction scratch is the file-scope device array below, so the
 // call itself issues no allocation or free of any kind.
 //
-// The array (~2.7 MB) is held by every GPU that loads this library until
-// the process exits.  Every call shares it and it keeps the last call's
+// The array (~2.7 MB) is held until the process exits by every GPU on which
+// the module holding it is loaded.  With CUDA's lazy module loading (the
+// default since CUDA 12.2) that happens at the first call on each device:
+// that call loads the module, which allocates the array and may synchronise
+// the device, so callers make one warm-up call (k = 0 will do) per device at
+// start-up, before any stream capture.  Every call shares it and it keeps the last call's
 // contents, so the call clears what must start at zero (the completion
 // counter of the norm reduction) before it launches, and two calls that
 // overlap on the GPU (different streams, or different host threads on one
@@ -81,6 +85,11 @@ extern "C" bbjd_status bbjd_dev_orthogonalize_static(bbjd_int n, bbjd_int k, con
     S.n = n;
     const int sms = num_sms();
     int G = (int)std::max<int64_t>(1, std::min<int64_t>(std::min(4 * sms, ST_G_MAX), (n + 255) / 256));
+    // the dot kernel stages its rows' v in shared memory (16 B a row): on a
+    // device with few SMs visible (MPS, green contexts) use all ST_G_MAX CTAs,
+    // which keeps n <= BBJD_STATIC_ORTH_MAX_N under 205 KB whatever the SM count
+    if (16 * (((n + G - 1) / G + 31) / 32 * 32) > 200 * 1024)
+        G = (int)std::max<int64_t>(1, std::min<int64_t>(ST_G_MAX, (n + 255) / 256));
     S.rpc = ((n + G - 1) / G + 31) / 32 * 32;
     S.G = (int)((n + S.rpc - 1) / S.rpc);
     S.G2 = (int)std::max<int64_t>(1, std::min<int64_t>(std::min(8 * sms, ST_G2_MAX), (n + 255) / 256));

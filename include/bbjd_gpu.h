@@ -200,13 +200,16 @@ bbjd_status bbjd_dev_orthogonalize(bbjd_int n, bbjd_int k, const bbjd_zomplex *Q
  * cudaMalloc there: a framework that owns all device memory and forbids
  * allocation after start-up, or a pipeline that must not stall the device
  * (cudaMalloc and cudaFree synchronise it).  Its reduction scratch is one
- * static device array of about 2.7 MB in the library, held by every GPU
- * that loads the library until exit.  Limits: n <= BBJD_STATIC_ORTH_MAX_N,
+ * static device array of about 2.7 MB in the library, held until exit by
+ * every GPU on which the library's module has been loaded.  Limits: n <= BBJD_STATIC_ORTH_MAX_N,
  * k <= BBJD_STATIC_ORTH_MAX_K; larger sizes return BBJD_ERR_INVALID with a
  * message on stderr.  The first call on each device looks the array up
- * (cudaGetSymbolAddress).  Calls share the array: two calls that overlap on
- * the GPU (other streams or host threads on the same device) race, so
- * serialise them.  Q and v are device pointers; *norm_out and
+ * (cudaGetSymbolAddress); under CUDA's lazy module loading (the default)
+ * that first call also loads the module holding the array, which allocates
+ * it and may synchronise the device, so make one warm-up call per device
+ * (k = 0 will do) at start-up, before any stream capture.  Calls share the
+ * array: two calls that overlap on the GPU (other streams or host threads
+ * on the same device) race, so serialise them.  Q and v are device pointers; *norm_out and
  * *second_pass_out are host. */
 #define BBJD_STATIC_ORTH_MAX_N 8388608
 #define BBJD_STATIC_ORTH_MAX_K 256

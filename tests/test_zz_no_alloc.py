@@ -50,6 +50,34 @@ def test_static_matches_allocating_twice(n, k):
         assert got_s == ref_s
 
 
+def test_static_allocates_nothing_after_warm_up():
+    """After one warm-up call (which, under lazy module loading, loads the
+    module holding the static scratch), a call leaves the device's free
+    memory unchanged, also at the largest size it accepts."""
+    import torch
+    lib = _lib.load()
+    for n, k in [(4104, 8), (MAX_N, 4)]:
+        Qd = torch.randn(k, n, dtype=torch.complex128, device="cuda")   # column-major n x k
+        Qd = torch.linalg.qr(Qd.T)[0].T.contiguous()
+        vd = torch.randn(n, dtype=torch.complex128, device="cuda")
+        ref = vd.clone()
+        nrm, second = C.c_double(), C.c_int()
+        call = lambda x: lib.bbjd_dev_orthogonalize_static(  # noqa: E731
+            n, k, Qd.data_ptr(), n, x.data_ptr(), C.byref(nrm), C.byref(second), None)
+        assert call(vd) == 0                      # warm-up
+        torch.cuda.synchronize()
+        free0 = torch.cuda.mem_get_info()[0]
+        vd.copy_(ref)
+        assert call(vd) == 0
+        torch.cuda.synchronize()
+        assert torch.cuda.mem_get_info()[0] == free0
+        # and the result is orthogonal to Q to FP64 accuracy
+        h = torch.mv(Qd.conj(), vd)
+        assert float(h.abs().max()) <= 1e-12 * float(ref.norm())
+        del Qd, vd, ref
+        torch.cuda.empty_cache()
+
+
 def test_static_rejects_sizes_beyond_its_scratch():
     lib = _lib.load()
     nrm, second = C.c_double(), C.c_int()
