@@ -674,6 +674,14 @@ bbjd_status axpby(Scratch &S, const cplx *a_dev, cplx a, const cplx *x, const cp
     return BBJD_SUCCESS;
 }
 
+bbjd_status axpby_n(int64_t count, cplx a, const cplx *x, cplx b, const cplx *y, cplx *out,
+                    cudaStream_t st) {
+    const int64_t g = std::min<int64_t>(8 * num_sms(), std::max<int64_t>(1, (count + 255) / 256));
+    k_axpby<<<(unsigned)g, 256, 0, st>>>(count, nullptr, a, x, nullptr, b, y, out);
+    BBJD_LAUNCH_CHECK();
+    return BBJD_SUCCESS;
+}
+
 bbjd_status svdv(Scratch &S, const cplx *dots, const cplx *z, const cplx *s, cplx *out,
                  cudaStream_t st) {
     k_svdv<<<S.G2, 256, 0, st>>>(S.n, dots, z, s, out);
@@ -761,23 +769,41 @@ bbjd_status to_c64(int64_t count, const cplx *in, float2 *out, cudaStream_t st) 
 }
 
 bbjd_status tsdot32(Scratch &S, int ncols, int64_t ld, const float2 *Q, const cplx *v, cplx *out,
-                    cudaStream_t st) {
+                    cudaStream_t st, const int *flag) {
     const int X = ncols + 1;
     if (X > S.maxX) return BBJD_ERR_INVALID;
     const size_t smem = sizeof(cplx) * (size_t)S.rpc;
     bbjd_status s = raise_smem_limit((const void *)k_tsdot<1, 1, float2>, smem);
     if (s) return s;
-    k_tsdot<1, 1, float2><<<S.G, 256, smem, st>>>(S.n, ncols, ld, Q, Q, v, nullptr, S.rpc, S.partial, nullptr);
+    k_tsdot<1, 1, float2><<<S.G, 256, smem, st>>>(S.n, ncols, ld, Q, Q, v, nullptr, S.rpc, S.partial, flag);
     BBJD_LAUNCH_CHECK();
-    return reduce_partials(S.partial, S.G, X, out, st);
+    k_reduce<<<(X + 31) / 32, 256, 0, st>>>(S.partial, S.G, X, out, flag);
+    BBJD_LAUNCH_CHECK();
+    return BBJD_SUCCESS;
 }
 
 bbjd_status update32(Scratch &S, int ncols, int64_t ld, const float2 *Q, const cplx *h, cplx *v,
-                     double *norm_out, cudaStream_t st) {
+                     double *norm_out, cudaStream_t st, const cplx *ref_nsq, int *flag_out,
+                     const int *flag_in) {
     const size_t smem = sizeof(cplx) * (size_t)std::max(ncols, 1);
     k_update<float2><<<S.G2, 256, smem, st>>>(S.n, ncols, ld, Q, h, nullptr, mk(1, 0), mk(0, 0), mk(1, 0),
                                               v, mk(0, 0), nullptr, v, S.nrm_part, S.counter, norm_out,
-                                              nullptr, nullptr, nullptr, nullptr);
+                                              ref_nsq, nullptr, flag_out, flag_in);
+    BBJD_LAUNCH_CHECK();
+    return BBJD_SUCCESS;
+}
+
+__global__ void k_cvt_c128(int64_t count, const float2 *__restrict__ in, double2 *__restrict__ out) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < count;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const float2 a = in[i];
+        out[i] = make_double2((double)a.x, (double)a.y);
+    }
+}
+
+bbjd_status to_c128(int64_t count, const float2 *in, cplx *out, cudaStream_t st) {
+    const int64_t g = std::min<int64_t>(8 * num_sms(), std::max<int64_t>(1, (count + 255) / 256));
+    k_cvt_c128<<<(unsigned)g, 256, 0, st>>>(count, in, out);
     BBJD_LAUNCH_CHECK();
     return BBJD_SUCCESS;
 }

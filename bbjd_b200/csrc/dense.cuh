@@ -54,6 +54,9 @@ bbjd_status scale_by_norm(Scratch &S, const cplx *v, const double *norm, double 
                           cplx *out, cudaStream_t st);
 bbjd_status axpby(Scratch &S, const cplx *a_dev, cplx a, const cplx *x, const cplx *b_dev, cplx b,
                   const cplx *y, cplx *out, cudaStream_t st);
+// out[0:count] = a x + b y (y may be null), host scalars.
+bbjd_status axpby_n(int64_t count, cplx a, const cplx *x, cplx b, const cplx *y, cplx *out,
+                    cudaStream_t st);
 bbjd_status svdv(Scratch &S, const cplx *dots, const cplx *z, const cplx *s, cplx *out,
                  cudaStream_t st);
 bbjd_status restart_gemm(int64_t n, int k, int keep, const cplx *X, int64_t ldx, const cplx *Z_dev,
@@ -71,12 +74,17 @@ bbjd_status gram(Scratch &S, int keep, const cplx *X, const cplx *Y, int64_t ldx
 bbjd_status to_row_major(int64_t r0, int64_t rows, int ncols, int64_t ld, const cplx *Q, cplx *out,
                          cudaStream_t st);
 
-// Mixed precision: out = complex64(in); the first CGS pass over a complex64
-// basis (dots into out[0:ncols], ||v||^2 into out[ncols]; v -= Q h).
+// Mixed precision: out = complex64(in) and back; a CGS pass over a complex64
+// basis Q with an FP64 vector v, FP64 accumulation (dots into out[0:ncols],
+// ||v||^2 into out[ncols]; v -= Q h, ||v|| into *norm_out and, with
+// ref_nsq / flag_out, the DGKS flag as update()).  Skipped when flag /
+// flag_in is set and *flag == 0.
 bbjd_status to_c64(int64_t count, const cplx *in, float2 *out, cudaStream_t st);
+bbjd_status to_c128(int64_t count, const float2 *in, cplx *out, cudaStream_t st);
 bbjd_status tsdot32(Scratch &S, int ncols, int64_t ld, const float2 *Q, const cplx *v, cplx *out,
-                    cudaStream_t st);
+                    cudaStream_t st, const int *flag = nullptr);
 bbjd_status update32(Scratch &S, int ncols, int64_t ld, const float2 *Q, const cplx *h, cplx *v,
-                     double *norm_out, cudaStream_t st);
+                     double *norm_out, cudaStream_t st, const cplx *ref_nsq = nullptr,
+                     int *flag_out = nullptr, const int *flag_in = nullptr);
 
 }  // namespace bbjd

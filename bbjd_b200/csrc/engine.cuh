@@ -106,6 +106,8 @@ struct Engine {
     int *dflag = nullptr;      // device flags
     bool mixed = false;        // BBJD_MIXED: complex64 shadow of V for the first CGS pass
     float2 *Vs = nullptr;      // n x maxsub complex64 copy of V (ld n)
+    float2 *gV32 = nullptr;    // BBJD_MIXED with inner GMRES: complex64 Arnoldi basis,
+                               // n x (inner_maxiter + 1) (ld n)
     int evec_layout = BBJD_EVEC_COLUMN_MAJOR;
     cplx *evd = nullptr;       // BBJD_EVEC_ROW_MAJOR: converged vectors, n x nev (ld n)
     cplx *pin = nullptr;       // pinned host staging for small results
@@ -178,7 +180,9 @@ struct Engine {
     bbjd_status orthogonalize_mixed(int k, cplx *v, double *norm_dev);
     bbjd_status project_out(const cplx *Q, int k, cplx *v, int cls);
     bbjd_status deflation_append(int j, const cplx *u, const cplx *Au_, const cplx *Bu_);
+    int rebuild_W_cholqr(int keep);
     bbjd_status gmres(int ndefl, zc ta, zc tb, const cplx *r, cplx *z);
+    bbjd_status gmres_mixed(int ndefl, zc ta, zc tb, const cplx *r, cplx *z);
     int solve_projected(int k, int locked, int nkeep, int *target_pos);
     int solve_projected_schur(int k, int nkeep, bool reorder, int *target_pos);
     void hessenberg_eigvec(int k, zc w, zc *x);

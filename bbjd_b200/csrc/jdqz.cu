@@ -49,6 +49,9 @@ void scipy_chseqr_(const char *job, const char *compz, const int *n, const int *
                    std::complex<float> *h, const int *ldh, std::complex<float> *w,
                    std::complex<float> *z, const int *ldz, std::complex<float> *work,
                    const int *lwork, int *info);
+void scipy_zpotrf_(const char *uplo, const int *n, bbjd_zomplex *a, const int *lda, int *info);
+void scipy_ztrtri_(const char *uplo, const char *diag, const int *n, bbjd_zomplex *a, const int *lda,
+                   int *info);
 void scipy_ztrsen_(const char *job, const char *compq, const int *select, const int *n,
                    bbjd_zomplex *t, const int *ldt, bbjd_zomplex *q, const int *ldq, bbjd_zomplex *w,
                    int *m, double *s, double *sep, bbjd_zomplex *work, const int *lwork, int *info);
@@ -243,6 +246,8 @@ bbjd_status Engine::init(const bbjd_params *p, bbjd_workspace *w, bbjd_result *r
     BBJD_CUDA_TRY(cudaMemset(dflag, 0, sizeof(int) * FL_N));
     mixed = e && e->precision == BBJD_MIXED;
     if (mixed) BBJD_CUDA_TRY(cudaMalloc(&Vs, sizeof(float2) * (size_t)n * maxsub));
+    if (mixed && p->inner_maxiter > 0)
+        BBJD_CUDA_TRY(cudaMalloc(&gV32, sizeof(float2) * (size_t)n * (p->inner_maxiter + 1)));
     evec_layout = e ? e->evec_layout : BBJD_EVEC_COLUMN_MAJOR;
     if (evec_layout == BBJD_EVEC_ROW_MAJOR) BBJD_CUDA_TRY(cudaMalloc(&evd, nv * (size_t)nev));
     const size_t pin_c = 8 * (size_t)(maxsub + nev + 8);
@@ -295,6 +300,8 @@ void Engine::release() {
     cudaFree(dscal); cudaFree(dflag);
     cudaFree(Vs);
     Vs = nullptr;
+    cudaFree(gV32);
+    gV32 = nullptr;
     cudaFree(evd);
     evd = nullptr;
     cudaFreeHost(pin); cudaFreeHost(pin_d); cudaFreeHost(pin_i);
@@ -1189,6 +1196,7 @@ static void zlartg_stable(zc f, zc g, double *cs, zc *sn, zc *r) {
 // same H column in exact arithmetic, two streaming passes over the basis
 // instead of 2(j+1) dependent BLAS-1 calls.
 bbjd_status Engine::gmres(int ndefl, zc ta, zc tb, const cplx *r, cplx *z) {
+    if (gV32) return gmres_mixed(ndefl, ta, tb, r, z);
     const int ims = (int)P->inner_maxiter;
     cplx *V = reinterpret_cast<cplx *>(ws->gmres_V);
     const cplx *Qr = reinterpret_cast<cplx *>(ws->Q_right);
@@ -1310,6 +1318,182 @@ bbjd_status Engine::gmres(int ndefl, zc ta, zc tb, const cplx *r, cplx *z) {
     T.end();
     bytes_dev += 16.0 * n * (m + 1.0);
     return project_out(Qr, ndefl, z, KC_GMRES);                     // jd_core.c:724
+}
+
+// The same GMRES with the Arnoldi basis in complex64 (BBJD_MIXED): each new
+// vector is formed in FP64 -- the projectors Q_l, Q_r, the products and the
+// preconditioner apply in FP64 (the preconditioner's factors may be
+// complex64) -- orthogonalised against the complex64 basis with FP64
+// accumulation (CGS + the same DGKS test), and stored in complex64, which
+// halves the Arnoldi traffic.  The Hessenberg matrix, the Givens rotations
+// and the least-squares solve stay FP64 on the host.  The basis is
+// orthonormal to complex64 accuracy (~1e-7), far below the inner tolerance
+// the correction needs; the outer iteration's FP64 residual test is
+// unchanged.
+bbjd_status Engine::gmres_mixed(int ndefl, zc ta, zc tb, const cplx *r, cplx *z) {
+    const int ims = (int)P->inner_maxiter;
+    float2 *V32 = gV32;
+    // FP64 work vectors: the new Arnoldi vector and the preconditioner input
+    // (the FP64 basis of the workspace is not used in this form)
+    cplx *wv = reinterpret_cast<cplx *>(ws->gmres_V), *pv = wv + n;
+    const cplx *Qr = reinterpret_cast<cplx *>(ws->Q_right);
+    const cplx *Ql = reinterpret_cast<cplx *>(ws->Q_left);
+    zc *H = ws->gmres_H, *sn = ws->gmres_sn, *g = ws->gmres_g;
+    double *cs = reinterpret_cast<double *>(ws->gmres_cs);
+    const double itol = P->inner_tol;
+    std::fill(H, H + (size_t)(ims + 1) * ims, zc(0));
+    bbjd_status s;
+    // v0 = -M^-1 P_L r
+    if ((s = axpby(S, nullptr, mk(-1, 0), r, nullptr, mk(0, 0), nullptr, g1, st))) return s;
+    if ((s = project_out(Ql, ndefl, g1, KC_GMRES))) return s;
+    if (ops->has_precond()) {
+        T.begin(KC_PRECOND, ops->precond_bytes(1));
+        s = ops->precond(1, g1, wv);
+        T.end();
+        bytes_dev += ops->precond_bytes(1);
+    } else {
+        s = cudaMemcpyAsync(wv, g1, sizeof(cplx) * n, cudaMemcpyDeviceToDevice, st) ? BBJD_ERR_CUDA : BBJD_SUCCESS;
+    }
+    if (s) return s;
+    s = update(S, 0, n, nullptr, nullptr, nullptr, mk(0, 0), mk(0, 0), mk(1, 0), wv, mk(0, 0), nullptr,
+               wv, dscal + SC_GNORM, nullptr, nullptr, nullptr, nullptr, st);
+    if (s) return s;
+    BBJD_CUDA_TRY(cudaMemcpyAsync(pin_d, dscal + SC_GNORM, sizeof(double), cudaMemcpyDeviceToHost, st));
+    if ((s = sync())) return s;
+    const double beta0 = pin_d[0];
+    if (beta0 < 1e-300) {
+        BBJD_CUDA_TRY(cudaMemsetAsync(z, 0, sizeof(cplx) * n, st));
+        return BBJD_SUCCESS;
+    }
+    if ((s = scale_by_norm(S, wv, dscal + SC_GNORM, 0.0, wv, st))) return s;
+    if ((s = to_c64(n, wv, V32, st))) return s;
+    std::fill(g, g + ims + 1, zc(0));
+    g[0] = beta0;
+    int j;
+    for (j = 0; j < ims; ++j) {
+        if ((s = to_c128(n, V32 + (int64_t)j * n, g1, st))) return s;
+        if ((s = project_out(Qr, ndefl, g1, KC_GMRES))) return s;
+        T.begin(KC_SPMV, ops->apply_bytes(true));
+        s = ops->apply(g1, g2, g3, C(ta), C(tb), wv, dscal + SC_TMP2);   // wv = tb A g1 - ta B g1
+        T.end();
+        bytes_dev += ops->apply_bytes(true);
+        if (s) return s;
+        if ((s = project_out(Ql, ndefl, wv, KC_GMRES))) return s;
+        if (ops->has_precond()) {
+            BBJD_CUDA_TRY(cudaMemcpyAsync(pv, wv, sizeof(cplx) * n, cudaMemcpyDeviceToDevice, st));
+            T.begin(KC_PRECOND, ops->precond_bytes(1));
+            s = ops->precond(1, pv, wv);
+            T.end();
+            bytes_dev += ops->precond_bytes(1);
+            if (s) return s;
+        }
+        // Arnoldi against the complex64 basis: CGS + DGKS, H column from both passes
+        const int kk = j + 1;
+        int *flag = dflag + FL_G;
+        const double pass_bytes = 8.0 * n * (2.0 * kk) + 16.0 * n * 3.0;
+        T.begin(KC_GMRES, pass_bytes);
+        if ((s = tsdot32(S, kk, n, V32, wv, S.red, st))) return s;
+        if ((s = update32(S, kk, n, V32, S.red, wv, dscal + SC_GNORM, st, S.red + kk, flag))) return s;
+        cplx *h2 = S.red + S.maxX;
+        BBJD_CUDA_TRY(cudaMemsetAsync(h2, 0, sizeof(cplx) * kk, st));
+        if ((s = tsdot32(S, kk, n, V32, wv, h2, st, flag))) return s;
+        if ((s = update32(S, kk, n, V32, h2, wv, dscal + SC_GNORM, st, nullptr, nullptr, flag))) return s;
+        T.end();
+        bytes_dev += pass_bytes;
+        BBJD_CUDA_TRY(cudaMemcpyAsync(pin, S.red, sizeof(cplx) * (kk + 1), cudaMemcpyDeviceToHost, st));
+        BBJD_CUDA_TRY(cudaMemcpyAsync(pin + kk + 1, h2, sizeof(cplx) * kk, cudaMemcpyDeviceToHost, st));
+        BBJD_CUDA_TRY(cudaMemcpyAsync(pin_d, dscal + SC_GNORM, sizeof(double), cudaMemcpyDeviceToHost, st));
+        BBJD_CUDA_TRY(cudaMemcpyAsync(pin_i, flag, sizeof(int), cudaMemcpyDeviceToHost, st));
+        if ((s = sync())) return s;
+        const double w_before = std::sqrt(pin[kk].x);
+        for (int i = 0; i < kk; ++i) {
+            zc h = Z(pin[i]);
+            if (pin_i[0]) h += Z(pin[kk + 1 + i]);
+            H[i + (size_t)j * (ims + 1)] = h;
+        }
+        if (pin_i[0]) {
+            dgks++;
+            T.bytes[KC_GMRES] += pass_bytes;
+            bytes_dev += pass_bytes;
+        }
+        const double hjj1 = pin_d[0];
+        H[(j + 1) + (size_t)j * (ims + 1)] = hjj1;
+        if (hjj1 < 1e-14 * w_before) { j++; break; }               // jd_core.c:674
+        if ((s = scale_by_norm(S, wv, dscal + SC_GNORM, 0.0, wv, st))) return s;
+        if ((s = to_c64(n, wv, V32 + (int64_t)(j + 1) * n, st))) return s;
+        for (int i = 0; i < j; ++i) {                               // jd_core.c:680-685
+            const zc h1 = H[i + (size_t)j * (ims + 1)], h2v = H[i + 1 + (size_t)j * (ims + 1)];
+            H[i + (size_t)j * (ims + 1)] = cs[i] * h1 + sn[i] * h2v;
+            H[i + 1 + (size_t)j * (ims + 1)] = -std::conj(sn[i]) * h1 + cs[i] * h2v;
+        }
+        double csj;
+        zc snj, rj;
+        zlartg_stable(H[j + (size_t)j * (ims + 1)], H[(j + 1) + (size_t)j * (ims + 1)], &csj, &snj, &rj);
+        cs[j] = csj;
+        sn[j] = snj;
+        H[j + (size_t)j * (ims + 1)] = rj;
+        H[j + 1 + (size_t)j * (ims + 1)] = 0.0;
+        const zc ga = g[j], gb = g[j + 1];
+        g[j] = cs[j] * ga + sn[j] * gb;
+        g[j + 1] = -std::conj(sn[j]) * ga + cs[j] * gb;
+        if (std::abs(g[j + 1]) < itol * beta0) { j++; break; }      // jd_core.c:705
+    }
+    const int m = j;
+    zc *y = g;                                                      // jd_core.c:711-716
+    for (int i = m - 1; i >= 0; --i) {
+        for (int k2 = i + 1; k2 < m; ++k2) y[i] -= H[i + (size_t)k2 * (ims + 1)] * y[k2];
+        if (std::abs(H[i + (size_t)i * (ims + 1)]) > 1e-300) y[i] /= H[i + (size_t)i * (ims + 1)];
+    }
+    // z = V_m y: z = 0 - V (-y)
+    for (int i = 0; i < m; ++i) pin[i] = C(-y[i]);
+    BBJD_CUDA_TRY(cudaMemcpyAsync(xdev, pin, sizeof(cplx) * std::max(m, 1), cudaMemcpyHostToDevice, st));
+    BBJD_CUDA_TRY(cudaMemsetAsync(z, 0, sizeof(cplx) * n, st));
+    T.begin(KC_GMRES, 8.0 * n * m + 32.0 * n);
+    if ((s = update32(S, m, n, V32, xdev, z, dscal + SC_TMP, st))) return s;
+    T.end();
+    bytes_dev += 8.0 * n * m + 32.0 * n;
+    return project_out(Qr, ndefl, z, KC_GMRES);                     // jd_core.c:724
+}
+
+// W[:, 0:keep] = orthonormal basis of nu0 AV[:, 0:keep] + mu0 BV[:, 0:keep]
+// by CholQR2: X = nu0 AV + mu0 BV, then twice G = X^H X (device Gram),
+// G = R^H R (ZPOTRF, host FP64), X = X R^-1 (device, in place).  0: done;
+// 1: a Cholesky factorisation failed (X too ill-conditioned; W is left for
+// the caller to rebuild column by column); -1: a CUDA error.
+int Engine::rebuild_W_cholqr(int keep) {
+    cplx *W = reinterpret_cast<cplx *>(ws->W);
+    const cplx *AV = reinterpret_cast<cplx *>(ws->AV), *BV = reinterpret_cast<cplx *>(ws->BV);
+    const int64_t ld = n;
+    T.begin(KC_RESTART, 48.0 * n * keep);
+    if (axpby_n(n * keep, C(nu0), AV, C(mu0), BV, W, st)) return -1;
+    T.end();
+    bytes_dev += 48.0 * n * keep;
+    std::vector<cplx> g((size_t)keep * keep);
+    std::vector<zc> R((size_t)keep * keep);
+    for (int pass = 0; pass < 2; ++pass) {
+        T.begin(KC_RESTART, 16.0 * n * keep);
+        if (gram(S, keep, W, W, ld, gram_part, gram_G, gram_out, st)) return -1;
+        T.end();
+        bytes_dev += 16.0 * n * keep;
+        if (cudaMemcpyAsync(g.data(), gram_out, sizeof(cplx) * keep * keep, cudaMemcpyDeviceToHost, st) ||
+            sync())
+            return -1;
+        for (size_t e = 0; e < g.size(); ++e) R[e] = Z(g[e]);
+        int info = 0;
+        scipy_zpotrf_("U", &keep, R.data(), &keep, &info);
+        if (info != 0) return 1;
+        scipy_ztrtri_("U", "N", &keep, R.data(), &keep, &info);
+        if (info != 0) return 1;
+        for (int j = 0; j < keep; ++j)
+            for (int i = 0; i < keep; ++i) g[i + (size_t)j * keep] = i <= j ? C(R[i + (size_t)j * keep]) : mk(0, 0);
+        if (cudaMemcpyAsync(Zdev, g.data(), sizeof(cplx) * keep * keep, cudaMemcpyHostToDevice, st)) return -1;
+        T.begin(KC_RESTART, 32.0 * n * keep);
+        if (restart_gemm(n, keep, keep, W, ld, Zdev, keep, W, st)) return -1;
+        T.end();
+        bytes_dev += 32.0 * n * keep;
+        if (sync()) return -1;      // g is reused by the next pass
+    }
+    return 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -1558,14 +1742,22 @@ bbjd_status Engine::run() {
             if ((s = restart_gemm(n, (int)k, (int)keep, BV, ld, Zdev, (int)k, BV, st))) return s;
             T.end();
             bytes_dev += 3 * gb;
-            // rebuild W from the kept test images (jd_core.c:1002-1010)
-            for (int64_t j = 0; j < keep; ++j) {
-                cplx *wj = W + j * ld;
-                if ((s = update(S, 0, ld, nullptr, nullptr, nullptr, mk(0, 0), mk(0, 0), C(nu0), AV + j * ld,
-                                C(mu0), BV + j * ld, wj, dscal + SC_TMP, nullptr, nullptr, nullptr, nullptr, st)))
-                    return s;
-                if ((s = orthogonalize(W, ld, (int)j, wj, dscal + SC_TMP, KC_RESTART))) return s;
-                if ((s = scale_by_norm(S, wj, dscal + SC_TMP, 1e-300, wj, st))) return s;
+            // rebuild W from the kept test images (jd_core.c:1002-1010): the
+            // orthonormal basis of nu0 AV + mu0 BV, by CholQR2 (two Gram
+            // passes, FP64 Cholesky on the host) -- the Q of Gram-Schmidt up
+            // to rounding, as both keep R's diagonal positive -- and column by
+            // column as the reference where a Cholesky factorisation fails
+            int cq = rebuild_W_cholqr((int)keep);
+            if (cq < 0) return res->status = BBJD_ERR_CUDA;
+            if (cq > 0) {
+                for (int64_t j = 0; j < keep; ++j) {
+                    cplx *wj = W + j * ld;
+                    if ((s = update(S, 0, ld, nullptr, nullptr, nullptr, mk(0, 0), mk(0, 0), C(nu0), AV + j * ld,
+                                    C(mu0), BV + j * ld, wj, dscal + SC_TMP, nullptr, nullptr, nullptr, nullptr, st)))
+                        return s;
+                    if ((s = orthogonalize(W, ld, (int)j, wj, dscal + SC_TMP, KC_RESTART))) return s;
+                    if ((s = scale_by_norm(S, wj, dscal + SC_TMP, 1e-300, wj, st))) return s;
+                }
             }
             // MA = W^H AV, MB = W^H BV (jd_core.c:1016-1026)
             T.begin(KC_RESTART, 3.0 * 16.0 * n * keep);

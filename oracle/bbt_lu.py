@@ -63,3 +63,27 @@ class BBTLUHost:
         if getattr(self, "_h", None):
             self._lib.bbt_lu_free(self._h)
             self._h = None
+
+
+class BlockJacobiHost:
+    """Block-Jacobi preconditioner of A - sigma B for a BBTPencil on the host
+    (test infrastructure): the inverses of the interior diagonal blocks
+    Ad_j - sigma Bd_j and of the t x t tau corner of A (B's tau rows are
+    zero), with the ``.solve(b)`` interface of the reference's
+    preconditioner argument (reference bbjd.py:125-127).  The same operator
+    as the device's block Jacobi."""
+
+    def __init__(self, pencil, sigma: complex):
+        s = complex(sigma)
+        self.b, self.nblk, self.nb, self.n = pencil.b, pencil.nblk, pencil.nb, pencil.n
+        self.Dinv = np.linalg.inv(pencil.Ad - s * pencil.Bd)
+        self.Ginv = np.linalg.inv(pencil.F[:, pencil.nb:]) if pencil.t else None
+
+    def solve(self, r):
+        r = np.asarray(r, dtype=np.complex128)
+        x = np.empty_like(r)
+        x[:self.nb] = np.einsum("jic,jc->ji", self.Dinv,
+                                r[:self.nb].reshape(self.nblk, self.b)).reshape(-1)
+        if self.Ginv is not None:
+            x[self.nb:] = self.Ginv @ r[self.nb:]
+        return x

@@ -9,7 +9,7 @@ shift-invert eigenvalues of the same pencils, as small ``.npz`` files here.
 Only this script reads the reference checkout; the fixtures it writes are
 what the tests read (the GPU box has no reference checkout).
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py [--ref REFERENCE_CHECKOUT] [--only case,...]
 """
 from __future__ import annotations
 
@@ -43,12 +43,16 @@ def _arpack(A, B, sigma, k):
 
 
 def bbt_case(name, b, nblk, t, sigma, k, maxsub, minsub, seed=0, inner_maxiter=0,
-             inner_tol=1e-2, pc_shift=0.0, maxiter=2000, n_arpack=None):
+             inner_tol=1e-2, pc_shift=0.0, maxiter=2000, n_arpack=None, pc="exact", v0_seed=None):
     from bbjd import jdqz  # the reference wrapper
     P = make_pencil(b, nblk, t, seed=seed)
     A, B = P.to_csc("A"), P.to_csc("B")
-    lu = _LU((A - (sigma + pc_shift) * B).tocsc())
-    v0 = start_vector(P.n, seed + 1)
+    if pc == "block_jacobi":
+        from oracle.bbt_lu import BlockJacobiHost
+        lu = BlockJacobiHost(P, sigma + pc_shift)
+    else:
+        lu = _LU((A - (sigma + pc_shift) * B).tocsc())
+    v0 = start_vector(P.n, seed + 1 if v0_seed is None else v0_seed)
     t0 = time.time()
     ev, evec, info = jdqz(A, B, k=k, sigma=sigma, tol=1e-10, maxiter=maxiter, maxsub=maxsub,
                           minsub=minsub, inner_maxiter=inner_maxiter, inner_tol=inner_tol,
@@ -66,6 +70,7 @@ def bbt_case(name, b, nblk, t, sigma, k, maxsub, minsub, seed=0, inner_maxiter=0
                     for j in range(info["nconv"])])
     out = dict(kind="bbt", b=b, nblk=nblk, t=t, seed=seed, sigma=sigma, k=k, maxsub=maxsub,
                minsub=minsub, inner_maxiter=inner_maxiter, inner_tol=inner_tol, pc_shift=pc_shift,
+               preconditioner=pc, v0_seed=seed + 1 if v0_seed is None else v0_seed,
                maxiter=maxiter, eigenvalues=ev, residuals=info["residuals"], unscaled_residuals=res,
                iters=info["iters"], nconv=info["nconv"], status=info["status"], arpack=arp,
                seconds=dt)
@@ -105,20 +110,51 @@ def random_case():
     print(f"random200: nconv={info['nconv']} iters={info['iters']}")
 
 
+# The sigma-sweep configuration scaled to CPU size: pencils of the same
+# generator (b = t = 16) with uneven n, each with its own sigma on Re = 3
+# (seeded draws), k = 4, maxsub 80, minsub 32.
+SWEEP = dict(b=16, t=16, k=4, maxsub=80, minsub=32, nblks=(120, 173, 236, 301),
+             im=(-31.7, -8.2, 12.9, 36.4))
+
+
+def sweep_cases():
+    for i, (nblk, im) in enumerate(zip(SWEEP["nblks"], SWEEP["im"])):
+        bbt_case(f"sweep_{i}", b=SWEEP["b"], nblk=nblk, t=SWEEP["t"], sigma=complex(3.0, im),
+                 k=SWEEP["k"], maxsub=SWEEP["maxsub"], minsub=SWEEP["minsub"], seed=100 + i,
+                 v0_seed=1 + i)
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("BBJD_REFERENCE", "/root/reference"),
+                    help="reference checkout (default: $BBJD_REFERENCE)")
+    ap.add_argument("--only", default=None, help="comma-separated case names")
     args = ap.parse_args()
     sys.path.insert(0, os.path.join(ROOT, "oracle", "_ref"))   # _bbjd_c built from the reference
     sys.path.insert(0, args.ref)                               # the reference's bbjd.py
     os.environ.setdefault("OMP_NUM_THREADS", "4")
-    bbt_case("bbt_n4104", b=16, nblk=256, t=8, sigma=3.0, k=8, maxsub=40, minsub=20)
-    bbt_case("bbt_n516", b=8, nblk=64, t=4, sigma=3.0, k=6, maxsub=30, minsub=12)
-    bbt_case("bbt_n516_gmres", b=8, nblk=64, t=4, sigma=3.0, k=3, maxsub=30, minsub=12,
-             inner_maxiter=20, inner_tol=1e-2, pc_shift=0.5, maxiter=600)
-    bbt_case("bbt_n1056_b32", b=32, nblk=32, t=32, sigma=3.0, k=6, maxsub=40, minsub=16, seed=3)
-    diag_case()
-    random_case()
+    cases = {
+        "bbt_n4104": lambda: bbt_case("bbt_n4104", b=16, nblk=256, t=8, sigma=3.0, k=8, maxsub=40,
+                                      minsub=20),
+        "bbt_n516": lambda: bbt_case("bbt_n516", b=8, nblk=64, t=4, sigma=3.0, k=6, maxsub=30,
+                                     minsub=12),
+        "bbt_n516_gmres": lambda: bbt_case("bbt_n516_gmres", b=8, nblk=64, t=4, sigma=3.0, k=3,
+                                           maxsub=30, minsub=12, inner_maxiter=20, inner_tol=1e-2,
+                                           pc_shift=0.5, maxiter=600),
+        "bbt_n1056_b32": lambda: bbt_case("bbt_n1056_b32", b=32, nblk=32, t=32, sigma=3.0, k=6,
+                                          maxsub=40, minsub=16, seed=3),
+        # the inner-GMRES configuration (block Jacobi, inner 50 / 1e-3, maxsub
+        # 120 / minsub 48) at a CPU-runnable size
+        "bbt_n8256_gmres_bj": lambda: bbt_case("bbt_n8256_gmres_bj", b=32, nblk=256, t=64,
+                                               sigma=3.0, k=4, maxsub=120, minsub=48,
+                                               inner_maxiter=50, inner_tol=1e-3,
+                                               pc="block_jacobi", maxiter=1500),
+        "sweep": sweep_cases,
+        "diag50": diag_case,
+        "random200": random_case,
+    }
+    for name in (args.only.split(",") if args.only else cases):
+        cases[name]()
 
 
 if __name__ == "__main__":

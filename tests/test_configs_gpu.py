@@ -1,0 +1,86 @@
+"""Parity of the device engine with the reference on the benchmark's other
+configurations, scaled to sizes the reference runs on the CPU
+(tests/golden, produced by tests/golden/make_golden.py):
+
+* the batched sigma-sweep: pencils of the same generator with uneven n,
+  each with its own sigma on Re = 3, solved together by ``jdqz_batch``;
+* the inner-GMRES configuration: block-Jacobi preconditioner, inner GMRES
+  of 50 steps to 1e-3, maxsub 120 / minsub 48.
+
+Every returned pair must lie within the conditioning-aware bound of
+tests/parity.py of an ARPACK eigenvalue, and match the reference's own pair
+for that eigenvalue within the same bound (the sweep: all but two of them,
+the set-overlap criterion, since two JDQZ runs whose paths part can return
+different sets of k among the eigenvalues near sigma)."""
+import os
+
+import numpy as np
+import pytest
+
+from bbjd_b200 import jdqz, jdqz_batch, make_pencil, start_vector
+from tests.parity import (assert_eigs_match, assert_no_duplicates, eig_bound, eig_condition, nearest,
+                          unscaled_residual)
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def _load(name):
+    return dict(np.load(os.path.join(GOLDEN, name + ".npz"), allow_pickle=False))
+
+
+def _pencil(g):
+    return make_pencil(int(g["b"]), int(g["nblk"]), int(g["t"]), seed=int(g["seed"]))
+
+
+def _same_set(P, ev, evecs, g, slack=0):
+    """Every value within its bound of an ARPACK value (the k + 16 nearest
+    sigma); all but `slack` of them also within the bound of the reference
+    run's own value for that eigenvalue (JDQZ does not always return the k
+    nearest, and two runs whose paths part can return different sets)."""
+    assert_eigs_match(P, ev, evecs, g["arpack"])
+    ref = g["eigenvalues"]
+    idx = nearest(ev, ref)
+    hits = 0
+    for j, (lam, x) in enumerate(zip(ev, evecs.T)):
+        i = idx[j]
+        kap = eig_condition(P, ref[i])
+        r = unscaled_residual(P, lam, x) + g["unscaled_residuals"][i]
+        hits += abs(lam - ref[i]) <= eig_bound(lam, kap, r)
+    assert hits >= len(ev) - slack, (ev, ref)
+    assert_no_duplicates(ev)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_sweep_matches_reference_per_pencil(precision):
+    gs = [_load(f"sweep_{i}") for i in range(4)]
+    pencils = [_pencil(g) for g in gs]
+    sigmas = [complex(g["sigma"]) for g in gs]
+    g0 = gs[0]
+    out, wall = jdqz_batch(pencils, sigmas, k=int(g0["k"]), tol=1e-10, maxiter=int(g0["maxiter"]),
+                           maxsub=int(g0["maxsub"]), minsub=int(g0["minsub"]),
+                           precision=precision, threads=4,
+                           v0s=[start_vector(P.n, int(g["v0_seed"])) for P, g in zip(pencils, gs)])
+    for P, g, (ev, evecs, info) in zip(pencils, gs, out):
+        assert info["nconv"] == int(g["k"])
+        for lam, x in zip(ev, evecs.T):
+            assert unscaled_residual(P, lam, x) < 1e-8
+        # the parity criterion for sets: overlap >= k - 2 with the reference's
+        _same_set(P, ev, evecs, g, slack=2)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_block_jacobi_gmres_matches_reference(precision):
+    g = _load("bbt_n8256_gmres_bj")
+    P = _pencil(g)
+    ev, evecs, info = jdqz(P, k=int(g["k"]), sigma=complex(g["sigma"]), tol=1e-10,
+                           maxiter=int(g["maxiter"]), maxsub=int(g["maxsub"]),
+                           minsub=int(g["minsub"]), inner_maxiter=int(g["inner_maxiter"]),
+                           inner_tol=float(g["inner_tol"]), preconditioner="block_jacobi",
+                           precision=precision, v0=start_vector(P.n, int(g["v0_seed"])),
+                           return_info=True)
+    assert info["nconv"] == int(g["k"]) and info["status"] == 0
+    assert np.all(info["residuals"] < 1e-10)
+    _same_set(P, ev, evecs, g)
+    # same algorithm: the outer iteration count follows the reference's
+    assert abs(info["iters"] - int(g["iters"])) <= max(10, 0.25 * int(g["iters"]))
