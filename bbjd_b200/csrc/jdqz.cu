@@ -107,6 +107,11 @@ const MklLapack &mkl_lapack() {
 namespace bbjd {
 
 static inline cplx C(zc z) { return mk(z.real(), z.imag()); }
+static bool finite_all(const zc *a, int64_t count) {
+    for (int64_t i = 0; i < count; ++i)
+        if (!std::isfinite(a[i].real()) || !std::isfinite(a[i].imag())) return false;
+    return true;
+}
 static inline zc Z(cplx c) { return zc(c.x, c.y); }
 
 // device scalar slots
@@ -1550,7 +1555,8 @@ bbjd_status Engine::run() {
         BBJD_CUDA_TRY(cudaMemcpyAsync(pin_d, dscal + SC_VNORM, sizeof(double), cudaMemcpyDeviceToHost, st));
         if ((s = sync())) return s;
     }
-    if (pin_d[0] < 1e-300) return res->status = BBJD_ERR_BREAKDOWN;
+    // a zero or non-finite start vector (NaN / Inf in v0) cannot start a solve
+    if (!(pin_d[0] >= 1e-300) || !std::isfinite(pin_d[0])) return res->status = BBJD_ERR_BREAKDOWN;
     if ((s = scale_by_norm(S, V, dscal + SC_VNORM, 0.0, V, st))) return s;
     if (mixed && (s = to_c64(n, V, Vs, st))) return s;
     T.begin(KC_SPMV, abytes);
@@ -1569,6 +1575,7 @@ bbjd_status Engine::run() {
     if ((s = sync())) return s;
     ws->MA[0] = std::conj(Z(pin[0]));
     ws->MB[0] = std::conj(Z(pin[1]));
+    if (!finite_all(ws->MA, 1) || !finite_all(ws->MB, 1)) return res->status = BBJD_ERR_BREAKDOWN;
     ws->kdim = 1;
 
     for (int64_t iter = 0; iter < P->maxiter; ++iter) {             // jd_core.c:823
@@ -1631,7 +1638,12 @@ bbjd_status Engine::run() {
         if (s) return s;
         BBJD_CUDA_TRY(cudaMemcpyAsync(pin_d, dscal, sizeof(double) * 2, cudaMemcpyDeviceToHost, st));
         if ((s = sync())) return s;
-        if (pin_d[SC_UNORM] < 1e-300) {
+        // a non-finite norm (NaN / Inf from an operator or the pencil) is a
+        // breakdown: no later step could recover from it
+        if (!(pin_d[SC_UNORM] >= 1e-300) || !std::isfinite(pin_d[SC_UNORM]) ||
+            !std::isfinite(pin_d[SC_RNORM])) {
+            if ((s = settle(&redo_it))) return s;
+            if (redo_it) goto redo;
             res->status = BBJD_ERR_BREAKDOWN;
             return res->status;
         }
@@ -1794,6 +1806,12 @@ bbjd_status Engine::run() {
         BBJD_CUDA_TRY(cudaMemcpyAsync(pin_i + FL_T, dflag + FL_T, sizeof(int), cudaMemcpyDeviceToHost, st));
         if ((s = sync())) return s;
         if (pin_i[FL_T]) { dgks++; second_pass_bytes(KC_ORTH, (int)k); }
+        if (!std::isfinite(pin_d[SC_VNORM])) {
+            if ((s = settle(&redo_it))) return s;
+            if (redo_it) goto redo;
+            res->iters = iter + 1;
+            return res->status = BBJD_ERR_BREAKDOWN;
+        }
         if (pin_d[SC_VNORM] < 1e-14) {
             if ((s = settle(&redo_it))) return s;
             if (redo_it) goto redo;
@@ -1863,6 +1881,11 @@ bbjd_status Engine::run() {
         for (int64_t i = 0; i <= k; ++i) {
             ws->MA[k + (size_t)i * maxsub] = std::conj(Z(pin[i]));
             ws->MB[k + (size_t)i * maxsub] = std::conj(Z(pin[k + 1 + i]));
+        }
+        if (!std::isfinite(pin_d[SC_WNORM]) || !finite_all(reinterpret_cast<const zc *>(pin), 2 * (k + 1)) ||
+            !finite_all(&ws->MA[(size_t)k * maxsub], k) || !finite_all(&ws->MB[(size_t)k * maxsub], k)) {
+            res->iters = iter + 1;
+            return res->status = BBJD_ERR_BREAKDOWN;
         }
         // the committed target starts the next iteration's guess (not after a
         // restart: its vector is in the basis the restart replaced)

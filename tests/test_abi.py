@@ -86,12 +86,64 @@ def test_struct_layouts_match_c():
             assert ctypes.sizeof(PYMAP[key]) == val, key
 
 
-def test_reference_header_layout_is_kept():
-    """The reference's own header compiles against our struct sizes: the
-    fields the reference declares (include/bbjd.h:114-224 there) keep their
-    order; our header only appends enum values."""
+REF_PROBE = r"""
+#include <stdio.h>
+#include <stddef.h>
+#include "bbjd.h"
+#define P(T, F) printf(#T "." #F " %zu\n", offsetof(T, F))
+int main(void) {
+    printf("params %zu\nresult %zu\nworkspace %zu\n", sizeof(bbjd_params), sizeof(bbjd_result),
+           sizeof(bbjd_workspace));
+    P(bbjd_params, n); P(bbjd_params, nev); P(bbjd_params, sigma); P(bbjd_params, target);
+    P(bbjd_params, tol); P(bbjd_params, maxiter); P(bbjd_params, maxsub); P(bbjd_params, minsub);
+    P(bbjd_params, inner_maxiter); P(bbjd_params, inner_tol); P(bbjd_params, matvec_A);
+    P(bbjd_params, matvec_B); P(bbjd_params, precond); P(bbjd_params, op_data);
+    P(bbjd_params, verbose); P(bbjd_params, v0);
+    P(bbjd_result, nconv); P(bbjd_result, eigenvalues); P(bbjd_result, eigenvectors);
+    P(bbjd_result, residuals); P(bbjd_result, iters); P(bbjd_result, status);
+    P(bbjd_workspace, n); P(bbjd_workspace, maxsub); P(bbjd_workspace, nev);
+    P(bbjd_workspace, V); P(bbjd_workspace, W); P(bbjd_workspace, AV); P(bbjd_workspace, BV);
+    P(bbjd_workspace, MA); P(bbjd_workspace, MB); P(bbjd_workspace, SA); P(bbjd_workspace, SB);
+    P(bbjd_workspace, ZA); P(bbjd_workspace, ZB); P(bbjd_workspace, nlock); P(bbjd_workspace, kdim);
+    P(bbjd_workspace, gmres_V); P(bbjd_workspace, gmres_H); P(bbjd_workspace, gmres_cs);
+    P(bbjd_workspace, gmres_sn); P(bbjd_workspace, gmres_g); P(bbjd_workspace, inner_maxiter);
+    P(bbjd_workspace, tmp1); P(bbjd_workspace, tmp4); P(bbjd_workspace, swap_nm);
+    P(bbjd_workspace, Q_right); P(bbjd_workspace, Q_left); P(bbjd_workspace, h_work);
+    printf("BBJD_SUCCESS %d BBJD_MAX_ITER %d BBJD_ERR_ALLOC %d BBJD_ERR_INVALID %d "
+           "BBJD_ERR_CALLBACK %d BBJD_ERR_LAPACK %d BBJD_ERR_BREAKDOWN %d\n",
+           BBJD_SUCCESS, BBJD_MAX_ITER, BBJD_ERR_ALLOC, BBJD_ERR_INVALID, BBJD_ERR_CALLBACK,
+           BBJD_ERR_LAPACK, BBJD_ERR_BREAKDOWN);
+    printf("targets %d %d %d %d %d %d %d\n", BBJD_TARGET_NEAREST, BBJD_TARGET_LARGEST_MAG,
+           BBJD_TARGET_SMALLEST_MAG, BBJD_TARGET_LARGEST_REAL, BBJD_TARGET_SMALLEST_REAL,
+           BBJD_TARGET_LARGEST_IMAG, BBJD_TARGET_SMALLEST_IMAG);
+    return 0;
+}
+"""
+
+
+def _probe(include_dir):
     with tempfile.TemporaryDirectory() as d:
         src = os.path.join(d, "p.c")
-        open(src, "w").write('#include "bbjd.h"\nint main(void){bbjd_params p; bbjd_params_init(&p); return 0;}\n')
-        subprocess.run(["gcc", "-std=c11", "-c", "-I", INCLUDE, src, "-o", os.path.join(d, "p.o")],
-                       check=True)
+        exe = os.path.join(d, "p")
+        open(src, "w").write(REF_PROBE)
+        subprocess.run(["gcc", "-std=c11", "-I", include_dir, src, "-o", exe], check=True)
+        return subprocess.run([exe], check=True, capture_output=True, text=True).stdout
+
+
+REFERENCE = os.environ.get("BBJD_REFERENCE", "/root/reference")
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(REFERENCE, "include", "bbjd.h")),
+                    reason="the reference checkout is not on this machine ($BBJD_REFERENCE)")
+def test_layouts_identical_to_the_reference_header():
+    """The same probe compiled against the reference's own include/bbjd.h
+    and against ours: every size, offset and enum value the reference
+    declares is identical (its include/bbjd.h:61-224)."""
+    assert _probe(os.path.join(REFERENCE, "include")) == _probe(INCLUDE)
+
+
+def test_reference_probe_compiles_against_our_header():
+    """Without the reference checkout (the GPU box), the probe of the
+    reference's declarations still compiles and runs against our header."""
+    out = _probe(INCLUDE)
+    assert "params" in out and "BBJD_ERR_BREAKDOWN -5" in out
