@@ -1860,7 +1860,9 @@ bbjd_status Engine::run() {
         BBJD_CUDA_TRY(cudaMemcpyAsync(pin, hAB, sizeof(cplx) * 2 * k, cudaMemcpyDeviceToHost, st));
         if ((s = sync())) return s;
         if (pin_i[FL_W]) { dgks++; second_pass_bytes(KC_PENCIL, (int)k); }
-        if (pin_d[SC_WNORM] < 1e-14) {                              // jd_core.c:1061-1064
+        const double wnorm = pin_d[SC_WNORM];
+        const bool w_breakdown = wnorm < 1e-14;
+        if (w_breakdown) {                                          // jd_core.c:1061-1064
             BBJD_CUDA_TRY(cudaMemcpyAsync(wnew, AVk, sizeof(cplx) * n, cudaMemcpyDeviceToDevice, st));
             if ((s = orthogonalize(W, ld, (int)k, wnew, dscal + SC_WNORM, KC_PENCIL))) return s;
         }
@@ -1869,21 +1871,38 @@ bbjd_status Engine::run() {
             ws->MB[i + (size_t)k * maxsub] = Z(pin[k + i]);
         }
         if ((s = scale_by_norm(S, wnew, dscal + SC_WNORM, 1e-300, wnew, st))) return s;
-        // row k: MA[k, 0:k+1] = W_k^H AV[:, 0:k+1], MB likewise (jd_core.c:1090-1103)
-        T.begin(KC_PENCIL, 16.0 * n * (2.0 * (k + 1) + 1.0));
-        if ((s = tsdot(S, 2, 1, (int)(k + 1), ld, AV, BV, wnew, nullptr, S.red, nullptr, st))) return s;
+        // row k: MA[k, 0:k+1] = W_k^H AV[:, 0:k+1], MB likewise (jd_core.c:1090-1103).
+        // W is the orthonormal basis of (nu0 A + mu0 B) V built column by
+        // column, so C = nu0 MA + mu0 MB = W^H (nu0 A + mu0 B) V is upper
+        // triangular with C[k, k] = the norm of w before its normalisation:
+        // in the harmonic form only MB's row is read from the device (one
+        // pass over BV instead of AV and BV) and MA's row follows,
+        // MA[k, j] = (C[k, j] - mu0 MB[k, j]) / nu0, equal to the computed row
+        // up to the rounding of W's orthogonality.  The QZ form, and a w
+        // that broke down (it is then an image of AV_k alone), read both.
+        const bool implied_row = proj_mode == BBJD_PROJ_SCHUR && !w_breakdown;
+        const int nm = implied_row ? 1 : 2;
+        T.begin(KC_PENCIL, 16.0 * n * (nm * (k + 1.0) + 1.0));
+        if ((s = implied_row ? tsdot(S, 1, 1, (int)(k + 1), ld, BV, nullptr, wnew, nullptr, S.red + (k + 1),
+                                     nullptr, st)
+                             : tsdot(S, 2, 1, (int)(k + 1), ld, AV, BV, wnew, nullptr, S.red, nullptr, st)))
+            return s;
         T.end();
-        bytes_dev += 16.0 * n * (2.0 * (k + 1) + 1.0);
+        bytes_dev += 16.0 * n * (nm * (k + 1.0) + 1.0);
         BBJD_CUDA_TRY(cudaMemcpyAsync(pin, S.red, sizeof(cplx) * 2 * (k + 1), cudaMemcpyDeviceToHost, st));
         if ((s = sync())) return s;
         if ((s = settle(&redo_it))) return s;
         if (redo_it) goto redo;
         for (int64_t i = 0; i <= k; ++i) {
-            ws->MA[k + (size_t)i * maxsub] = std::conj(Z(pin[i]));
-            ws->MB[k + (size_t)i * maxsub] = std::conj(Z(pin[k + 1 + i]));
+            const zc mb = std::conj(Z(pin[k + 1 + i]));
+            ws->MB[k + (size_t)i * maxsub] = mb;
+            ws->MA[k + (size_t)i * maxsub] =
+                implied_row ? ((i == k ? zc(wnorm) : zc(0.0)) - mu0 * mb) / nu0 : std::conj(Z(pin[i]));
         }
-        if (!std::isfinite(pin_d[SC_WNORM]) || !finite_all(reinterpret_cast<const zc *>(pin), 2 * (k + 1)) ||
-            !finite_all(&ws->MA[(size_t)k * maxsub], k) || !finite_all(&ws->MB[(size_t)k * maxsub], k)) {
+        bool row_ok = std::isfinite(pin_d[SC_WNORM]);
+        for (int64_t i = 0; i <= k && row_ok; ++i)
+            row_ok = finite_all(&ws->MA[k + (size_t)i * maxsub], 1) && finite_all(&ws->MB[k + (size_t)i * maxsub], 1);
+        if (!row_ok || !finite_all(&ws->MA[(size_t)k * maxsub], k) || !finite_all(&ws->MB[(size_t)k * maxsub], k)) {
             res->iters = iter + 1;
             return res->status = BBJD_ERR_BREAKDOWN;
         }
