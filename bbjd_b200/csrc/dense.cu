@@ -218,8 +218,9 @@ __global__ void __launch_bounds__(256) k_update(
 // re-pass reads Q twice more (dots, then the update); with it once.
 //
 // One persistent CTA of 16 warps per SM walks tiles of 32 rows.  A tile's
-// 32 x ncols slice of Q is copied to shared memory by cp.async, double-
-// buffered (the next tile is in flight while this one is used).  Warp w
+// 32 x ncols slice of Q is copied to shared memory by cp.async into a ring
+// of NST buffers (NST - 1 tiles in flight while one is used; three where
+// they fit in shared memory, ncols <= 143, else two).  Warp w
 // owns columns w, w + 16, ... and lane l row l of the tile: the warps'
 // partial sums of Q h meet in shared memory, warp 0 forms v_out for the 32
 // rows (it alone reads v_in and writes v_out, which may alias), and every
@@ -231,8 +232,13 @@ constexpr int UD_CPW = 14;         // columns per warp: ncols <= 224
 constexpr int UD_MIN_COLS = 64;    // below, the separate dot pass is as cheap
 constexpr size_t UD_SMEM_LIMIT = 231424;
 
-static size_t update_dot_smem(int ncols) {
-    return sizeof(cplx) * ((size_t)2 * ncols * UD_TR + ncols + UD_WARPS * UD_TR + UD_TR);
+static size_t update_dot_smem(int ncols, int stages = 2) {
+    return sizeof(cplx) * ((size_t)stages * ncols * UD_TR + ncols + UD_WARPS * UD_TR + UD_TR);
+}
+// Three tile buffers (two tiles in flight while one is used) where they fit
+// in shared memory (ncols <= 143), else two.
+static int update_dot_stages(int ncols) {
+    return update_dot_smem(ncols, 3) <= UD_SMEM_LIMIT ? 3 : 2;
 }
 
 bool update_dot_fits(int ncols) {
@@ -246,6 +252,7 @@ __device__ __forceinline__ void cp_async16(void *smem, const void *gmem, int src
                  : "memory");
 }
 
+template <int NST>
 __global__ void __launch_bounds__(UD_WARPS * 32, 1) k_update_dot(
     int64_t n, int ncols, int64_t ld, const cplx *__restrict__ Q, const cplx *__restrict__ h1,
     const cplx *__restrict__ h2, cplx c1, cplx c2, cplx a, const cplx *v_in, cplx b,
@@ -254,8 +261,8 @@ __global__ void __launch_bounds__(UD_WARPS * 32, 1) k_update_dot(
     int *flag_out) {
     extern __shared__ cplx ud_smem[];
     const int per = ncols * UD_TR;
-    cplx *Qs = ud_smem;                         // two tiles, [ncols][UD_TR] each
-    cplx *hs = Qs + 2 * per;                    // c1 h1 + c2 h2
+    cplx *Qs = ud_smem;                         // NST tiles, [ncols][UD_TR] each
+    cplx *hs = Qs + NST * per;                  // c1 h1 + c2 h2
     cplx *red = hs + ncols;                     // [UD_WARPS][UD_TR] partial sums of Q h
     cplx *vs = red + UD_WARPS * UD_TR;          // the tile's v_out
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -274,7 +281,6 @@ __global__ void __launch_bounds__(UD_WARPS * 32, 1) k_update_dot(
             const bool in = row < n;
             cp_async16(dst + e, Q + (int64_t)j * ld + (in ? row : 0), in ? 16 : 0);
         }
-        asm volatile("cp.async.commit_group;\n" ::: "memory");
     };
     cplx acc[UD_CPW];
 #pragma unroll
@@ -282,12 +288,25 @@ __global__ void __launch_bounds__(UD_WARPS * 32, 1) k_update_dot(
     double nsq = 0.0;
     int buf = 0;
     int64_t tile = blockIdx.x;
-    if (tile < ntiles) issue(tile, Qs);
+    // prologue: the first NST - 1 tiles, one commit group each (possibly
+    // empty, so the group count stays in step with the tiles)
+#pragma unroll
+    for (int p = 0; p < NST - 1; ++p) {
+        const int64_t t = tile + (int64_t)p * gridDim.x;
+        if (t < ntiles) issue(t, Qs + p * per);
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    }
     for (; tile < ntiles; tile += gridDim.x) {
-        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-        __syncthreads();                        // tile landed; the other buffer is free
-        const int64_t next = tile + gridDim.x;
-        if (next < ntiles) issue(next, Qs + (buf ^ 1) * per);
+        // all but the newest NST - 2 groups complete: this tile has landed
+        if constexpr (NST == 3)
+            asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+        else
+            asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+        __syncthreads();                        // tile landed; the buffer used last is free
+        const int64_t next = tile + (int64_t)(NST - 1) * gridDim.x;
+        const int nbuf = buf + NST - 1 >= NST ? buf - 1 : buf + NST - 1;
+        if (next < ntiles) issue(next, Qs + nbuf * per);
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
         const cplx *Qt = Qs + buf * per;
         const int64_t row = tile * UD_TR + lane;
         cplx base = mk(0.0, 0.0);
@@ -320,8 +339,9 @@ __global__ void __launch_bounds__(UD_WARPS * 32, 1) k_update_dot(
             const int j = warp + UD_WARPS * c;
             if (j < ncols) cfmac(acc[c], Qt[j * UD_TR + lane], vo);
         }
-        buf ^= 1;
+        buf = buf + 1 == NST ? 0 : buf + 1;
     }
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     cplx *out = partial + (int64_t)blockIdx.x * (ncols + 1);
 #pragma unroll
     for (int c = 0; c < UD_CPW; ++c) {
@@ -579,7 +599,8 @@ bbjd_status Scratch::init(int64_t n_, int max_cols, int nvec) {
     BBJD_CUDA_TRY(cudaMemset(flags, 0, sizeof(int) * 16));
     // the fused CGS update stages tiles of the basis in up to 226 KB
     bbjd_status s;
-    if ((s = raise_smem_limit((const void *)k_update_dot, UD_SMEM_LIMIT))) return s;
+    if ((s = raise_smem_limit((const void *)k_update_dot<2>, UD_SMEM_LIMIT))) return s;
+    if ((s = raise_smem_limit((const void *)k_update_dot<3>, UD_SMEM_LIMIT))) return s;
     const size_t smem_need = sizeof(cplx) * 2 * (size_t)rpc;
     if ((s = raise_smem_limit((const void *)k_tsdot<1, 2>, smem_need))) return s;
     if ((s = raise_smem_limit((const void *)k_tsdot<2, 1>, smem_need))) return s;
@@ -643,9 +664,14 @@ bbjd_status cgs_tail(Scratch &S, int ncols, int64_t ld, const cplx *Q, const cpl
         const int64_t ntiles = (S.n + UD_TR - 1) / UD_TR;
         const int G = (int)std::max<int64_t>(1, std::min<int64_t>({(int64_t)num_sms(), ntiles,
                                                                     (int64_t)S.G}));
-        k_update_dot<<<G, UD_WARPS * 32, update_dot_smem(ncols), st>>>(
-            S.n, ncols, ld, Q, h1, h2, c1, c2, a, v_in, b, w_in, v_out, S.partial, S.nrm_part,
-            S.counter, norm_out, ref_nsq, ref_nrm, flag);
+        if (update_dot_stages(ncols) == 3)
+            k_update_dot<3><<<G, UD_WARPS * 32, update_dot_smem(ncols, 3), st>>>(
+                S.n, ncols, ld, Q, h1, h2, c1, c2, a, v_in, b, w_in, v_out, S.partial, S.nrm_part,
+                S.counter, norm_out, ref_nsq, ref_nrm, flag);
+        else
+            k_update_dot<2><<<G, UD_WARPS * 32, update_dot_smem(ncols, 2), st>>>(
+                S.n, ncols, ld, Q, h1, h2, c1, c2, a, v_in, b, w_in, v_out, S.partial, S.nrm_part,
+                S.counter, norm_out, ref_nsq, ref_nrm, flag);
         BBJD_LAUNCH_CHECK();
         k_reduce<<<(ncols + 1 + 31) / 32, 256, 0, st>>>(S.partial, G, ncols + 1, h_re, flag);
         BBJD_LAUNCH_CHECK();
