@@ -218,22 +218,34 @@ __global__ void __launch_bounds__(256) k_update(
 // re-pass reads Q twice more (dots, then the update); with it once.
 //
 // One persistent CTA of 16 warps per SM walks tiles of 32 rows.  A tile's
-// 32 x ncols slice of Q is copied to shared memory by cp.async into a ring
-// of NST buffers (NST - 1 tiles in flight while one is used; three where
-// they fit in shared memory, ncols <= 143, else two).  Warp w
-// owns columns w, w + 16, ... and lane l row l of the tile: the warps'
-// partial sums of Q h meet in shared memory, warp 0 forms v_out for the 32
-// rows (it alone reads v_in and writes v_out, which may alias), and every
-// lane accumulates conj(Q) v_out for its columns in registers across tiles;
-// the warp sums happen once, at the end.  Summation orders are fixed.
-constexpr int UD_TR = 32;          // rows per tile (lane = row)
+// 32 x ncols slice of Q, and its 32 rows of v_in and w_in, are copied to
+// shared memory by cp.async into a ring of NST buffers (NST - 1 tiles in
+// flight while one is used; three where they fit, ncols <= 143, else two).
+// A tile's column j sits at j * 33 (one 16-byte pad per column), so a warp
+// reading one row across 32 columns and a warp reading one column across
+// 32 rows both touch every bank group equally.  Two phases per tile, two
+// barriers:
+//   1. warp w forms rows w and w + 16: each lane sums Q[row, j] h[j] over
+//      its columns j = lane + 32 c (h held in registers), a butterfly warp
+//      sum gives the row's (Q h)[row], and v_out[row] = a v_in + b w_in -
+//      (Q h)[row] goes to global memory and to the tile's v_out in shared
+//      memory;
+//   2. warp w owns columns w, w + 16, ... and lane l row l: every lane
+//      accumulates conj(Q) v_out for its columns in registers across tiles;
+//      the warp sums happen once, at the end.
+// Summation orders are fixed (no atomics on values).
+constexpr int UD_TR = 32;          // rows per tile
+constexpr int UD_LD = UD_TR + 1;   // shared-memory stride of a tile column
 constexpr int UD_WARPS = 16;
-constexpr int UD_CPW = 14;         // columns per warp: ncols <= 224
+constexpr int UD_CPW = 14;         // phase-2 columns per warp: ncols <= 224
+constexpr int UD_HPL = 7;          // phase-1 columns per lane: ncols <= 224
 constexpr int UD_MIN_COLS = 64;    // below, the separate dot pass is as cheap
 constexpr size_t UD_SMEM_LIMIT = 231424;
 
+// one ring buffer: the Q tile, then 32 rows of v_in and of w_in
+__host__ __device__ inline size_t update_dot_stage(int ncols) { return (size_t)ncols * UD_LD + 2 * UD_TR; }
 static size_t update_dot_smem(int ncols, int stages = 2) {
-    return sizeof(cplx) * ((size_t)stages * ncols * UD_TR + ncols + UD_WARPS * UD_TR + UD_TR);
+    return sizeof(cplx) * ((size_t)stages * update_dot_stage(ncols) + UD_TR + UD_WARPS);
 }
 // Three tile buffers (two tiles in flight while one is used) where they fit
 // in shared memory (ncols <= 143), else two.
@@ -242,7 +254,7 @@ static int update_dot_stages(int ncols) {
 }
 
 bool update_dot_fits(int ncols) {
-    return ncols >= UD_MIN_COLS && ncols <= UD_WARPS * UD_CPW &&
+    return ncols >= UD_MIN_COLS && ncols <= UD_WARPS * UD_CPW && ncols <= 32 * UD_HPL &&
            update_dot_smem(ncols) <= UD_SMEM_LIMIT;
 }
 
@@ -260,26 +272,42 @@ __global__ void __launch_bounds__(UD_WARPS * 32, 1) k_update_dot(
     unsigned *counter, double *norm_out, const cplx *ref_nsq, const double *ref_nrm,
     int *flag_out) {
     extern __shared__ cplx ud_smem[];
-    const int per = ncols * UD_TR;
-    cplx *Qs = ud_smem;                         // NST tiles, [ncols][UD_TR] each
-    cplx *hs = Qs + NST * per;                  // c1 h1 + c2 h2
-    cplx *red = hs + ncols;                     // [UD_WARPS][UD_TR] partial sums of Q h
-    cplx *vs = red + UD_WARPS * UD_TR;          // the tile's v_out
+    const int per = (int)update_dot_stage(ncols);
+    const int qper = ncols * UD_LD;
+    cplx *ring = ud_smem;                       // NST x [Q tile | v_in rows | w_in rows]
+    cplx *vs = ring + NST * per;                // the tile's v_out
+    double *wn = reinterpret_cast<double *>(vs + UD_TR);   // per-warp ||v_out||^2
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    for (int j = tid; j < ncols; j += blockDim.x) {
-        cplx h = cmul(c1, h1[j]);
-        if (h2) cfma(h, c2, h2[j]);
-        hs[j] = h;
+    // phase-1 coefficients of this lane's columns
+    cplx hr[UD_HPL];
+#pragma unroll
+    for (int c = 0; c < UD_HPL; ++c) {
+        const int j = lane + 32 * c;
+        cplx h = mk(0.0, 0.0);
+        if (j < ncols) {
+            h = cmul(c1, h1[j]);
+            if (h2) cfma(h, c2, h2[j]);
+        }
+        hr[c] = h;
     }
     const int64_t ntiles = (n + UD_TR - 1) / UD_TR;
     // rows past n are zero-filled (source size 0), so they add nothing
     auto issue = [&](int64_t tile, cplx *dst) {
         const int64_t row0 = tile * UD_TR;
-        for (int e = tid; e < per; e += blockDim.x) {
+        for (int e = tid; e < ncols * UD_TR; e += blockDim.x) {
             const int j = e >> 5, r = e & 31;
             const int64_t row = row0 + r;
             const bool in = row < n;
-            cp_async16(dst + e, Q + (int64_t)j * ld + (in ? row : 0), in ? 16 : 0);
+            cp_async16(dst + j * UD_LD + r, Q + (int64_t)j * ld + (in ? row : 0), in ? 16 : 0);
+        }
+        if (tid < 2 * UD_TR) {
+            const cplx *src = tid < UD_TR ? v_in : w_in;
+            const int r = tid & (UD_TR - 1);
+            const int64_t row = row0 + r;
+            if (src) {
+                const bool in = row < n;
+                cp_async16(dst + qper + tid, src + (in ? row : 0), in ? 16 : 0);
+            }
         }
     };
     cplx acc[UD_CPW];
@@ -293,7 +321,7 @@ __global__ void __launch_bounds__(UD_WARPS * 32, 1) k_update_dot(
 #pragma unroll
     for (int p = 0; p < NST - 1; ++p) {
         const int64_t t = tile + (int64_t)p * gridDim.x;
-        if (t < ntiles) issue(t, Qs + p * per);
+        if (t < ntiles) issue(t, ring + p * per);
         asm volatile("cp.async.commit_group;\n" ::: "memory");
     }
     for (; tile < ntiles; tile += gridDim.x) {
@@ -302,42 +330,45 @@ __global__ void __launch_bounds__(UD_WARPS * 32, 1) k_update_dot(
             asm volatile("cp.async.wait_group 1;\n" ::: "memory");
         else
             asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-        __syncthreads();                        // tile landed; the buffer used last is free
+        __syncthreads();    // tile landed everywhere; the buffer and vs of the last tile are free
         const int64_t next = tile + (int64_t)(NST - 1) * gridDim.x;
         const int nbuf = buf + NST - 1 >= NST ? buf - 1 : buf + NST - 1;
-        if (next < ntiles) issue(next, Qs + nbuf * per);
+        if (next < ntiles) issue(next, ring + nbuf * per);
         asm volatile("cp.async.commit_group;\n" ::: "memory");
-        const cplx *Qt = Qs + buf * per;
-        const int64_t row = tile * UD_TR + lane;
-        cplx base = mk(0.0, 0.0);
-        if (warp == 0 && row < n) {
-            if (v_in) base = cmul(a, v_in[row]);
-            if (w_in) cfma(base, b, w_in[row]);
-        }
-        cplx p = mk(0.0, 0.0);
+        const cplx *Qt = ring + buf * per;
+        const int64_t row0 = tile * UD_TR;
+        // phase 1: rows warp and warp + 16
 #pragma unroll
-        for (int c = 0; c < UD_CPW; ++c) {
-            const int j = warp + UD_WARPS * c;
-            if (j < ncols) cfma(p, Qt[j * UD_TR + lane], hs[j]);
-        }
-        red[warp * UD_TR + lane] = p;
-        __syncthreads();
-        if (warp == 0) {
-            cplx sum = red[lane];
-            for (int w = 1; w < UD_WARPS; ++w) sum = cadd(sum, red[w * UD_TR + lane]);
-            const cplx vo = row < n ? csub(base, sum) : mk(0.0, 0.0);
-            vs[lane] = vo;
-            if (row < n) {
-                v_out[row] = vo;
-                nsq += cabs2(vo);
+        for (int q = 0; q < 2; ++q) {
+            const int r = warp + UD_WARPS * q;
+            cplx p = mk(0.0, 0.0);
+#pragma unroll
+            for (int c = 0; c < UD_HPL; ++c) {
+                const int j = lane + 32 * c;
+                if (j < ncols) cfma(p, Qt[j * UD_LD + r], hr[c]);
+            }
+            p = warp_sum(p);
+            if (lane == 0) {
+                const int64_t row = row0 + r;
+                cplx vo = mk(0.0, 0.0);
+                if (row < n) {
+                    cplx base = mk(0.0, 0.0);
+                    if (v_in) base = cmul(a, Qt[qper + r]);
+                    if (w_in) cfma(base, b, Qt[qper + UD_TR + r]);
+                    vo = csub(base, p);
+                    v_out[row] = vo;
+                    nsq += cabs2(vo);
+                }
+                vs[r] = vo;
             }
         }
         __syncthreads();
+        // phase 2: conj(Q) v_out for this warp's columns, lane = row
         const cplx vo = vs[lane];
 #pragma unroll
         for (int c = 0; c < UD_CPW; ++c) {
             const int j = warp + UD_WARPS * c;
-            if (j < ncols) cfmac(acc[c], Qt[j * UD_TR + lane], vo);
+            if (j < ncols) cfmac(acc[c], Qt[j * UD_LD + lane], vo);
         }
         buf = buf + 1 == NST ? 0 : buf + 1;
     }
@@ -349,10 +380,13 @@ __global__ void __launch_bounds__(UD_WARPS * 32, 1) k_update_dot(
         const cplx sum = warp_sum(acc[c]);
         if (lane == 0 && j < ncols) out[j] = sum;
     }
+    if (lane == 0) wn[warp] = nsq;
+    __syncthreads();
     __shared__ bool last;
     if (warp == 0) {
-        const double t = warp_sum(nsq);
         if (lane == 0) {
+            double t = 0.0;
+            for (int w = 0; w < UD_WARPS; ++w) t += wn[w];
             out[ncols] = mk(t, 0.0);
             nrm_part[blockIdx.x] = t;
             __threadfence();

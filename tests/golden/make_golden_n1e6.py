@@ -24,7 +24,7 @@ solved on the CPU by:
 Both take hours on a few cores, so their output is cached as
 ``tests/golden/bbt_n1000064.npz``; the GPU tests and ``bench.py`` read it.
 
-    python tests/golden/make_golden_n1e6.py [--maxiter 2000] [--threads 6]
+    python tests/golden/make_golden_n1e6.py [--maxiter 2000] [--threads 6] [--procs 4]
 """
 from __future__ import annotations
 
@@ -145,14 +145,27 @@ def run_arpack(n_arpack: int, threads: int) -> dict:
     return dict(arpack=lam, arpack_residuals=res, arpack_seconds=time.time() - t0)
 
 
-def run_kappa(lams, threads: int) -> dict:
-    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+def _kappa_chunk(lams):
     from bbjd_b200.pencils import make_pencil
     from tests.parity import eig_condition
     c = CASE
     P = make_pencil(c["b"], c["nblk"], c["t"], seed=0)
+    return [eig_condition(P, lam) for lam in lams]
+
+
+def run_kappa(lams, threads: int, procs: int = 1) -> dict:
+    """Condition numbers of `lams`, split over `procs` processes (spawned:
+    each builds the pencil and factors its own LUs, ~10 GB each)."""
+    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
     t0 = time.time()
-    kap = np.array([eig_condition(P, lam) for lam in lams])
+    lams = np.asarray(lams)
+    if procs <= 1:
+        kap = np.array(_kappa_chunk(lams))
+    else:
+        import multiprocessing as mp
+        chunks = [c for c in np.array_split(lams, procs) if len(c)]
+        with mp.get_context("spawn").Pool(len(chunks)) as pool:
+            kap = np.concatenate([np.asarray(k) for k in pool.map(_kappa_chunk, chunks)])
     print(f"  kappa of {len(lams)} values in {time.time() - t0:.0f} s: "
           f"{kap.min():.1f} .. {kap.max():.1f}", flush=True)
     return dict(arpack_kappa=kap)
@@ -163,6 +176,7 @@ def main():
     ap.add_argument("--maxiter", type=int, default=2000)
     ap.add_argument("--threads", type=int, default=6)
     ap.add_argument("--n-arpack", type=int, default=80)
+    ap.add_argument("--procs", type=int, default=1, help="processes for the condition numbers")
     ap.add_argument("--only", choices=["reference", "arpack", "kappa"], default=None)
     ap.add_argument("--child", default=None)
     args = ap.parse_args()
@@ -178,7 +192,7 @@ def main():
         out.update(run_arpack(args.n_arpack, args.threads))
         np.savez(OUT, **out)
     if args.only in (None, "kappa"):
-        out.update(run_kappa(out["arpack"], args.threads))
+        out.update(run_kappa(out["arpack"], args.threads, args.procs))
         np.savez(OUT, **out)
     print(f"wrote {OUT}")
 

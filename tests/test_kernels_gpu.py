@@ -113,15 +113,16 @@ def test_block_jacobi_matches_host(b, nblk, t):
     assert np.linalg.norm(_host(xd) - ref) / np.linalg.norm(ref) < 1e-12
 
 
-# 64 <= k <= 214: the update and the re-pass dots share one read of Q
-# (cgs_tail's fused kernel); other k take the separate dot pass.
+# 64 <= k <= 216: the update and the re-pass dots share one read of Q
+# (cgs_tail's fused kernel: three tile buffers up to k = 143, two above);
+# other k take the separate dot pass.
 # repass=False: v has no large component along Q, so the DGKS flag stays
 # down and the re-pass is skipped.
 @pytest.mark.parametrize("n,k,repass", [(1000, 0, True), (1000, 1, True), (4104, 37, True),
                                         (100003, 200, True), (50, 50, True), (70, 64, True),
-                                        (7001, 105, True), (7001, 106, True), (7001, 214, True),
-                                        (7001, 215, True), (70001, 120, False), (2000, 100, False),
-                                        (33, 5, False)])
+                                        (7001, 105, True), (7001, 143, True), (7001, 144, True),
+                                        (7001, 216, True), (7001, 217, True), (70001, 120, False),
+                                        (2000, 100, False), (33, 5, False), (100003, 64, True)])
 def test_orthogonalize_matches_oracle(n, k, repass):
     import torch
     rng = np.random.default_rng(n + k)
