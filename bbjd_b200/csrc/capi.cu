@@ -474,12 +474,21 @@ bbjd_status bbjd_dev_restart_gemm(bbjd_int n, bbjd_int k, bbjd_int keep, const b
     std::vector<cplx> zh((size_t)k * keep);
     for (bbjd_int c = 0; c < keep; ++c)
         for (bbjd_int i = 0; i < k; ++i) zh[c * k + i] = mk(Z_host[i + c * ldz].real(), Z_host[i + c * ldz].imag());
+    int *derr = nullptr;
     BBJD_CUDA_TRY(cudaMalloc(&dZ, sizeof(cplx) * zh.size()));
+    BBJD_CUDA_TRY(cudaMalloc(&derr, sizeof(int)));
+    BBJD_CUDA_TRY(cudaMemset(derr, 0, sizeof(int)));
     BBJD_CUDA_TRY(cudaMemcpy(dZ, zh.data(), sizeof(cplx) * zh.size(), cudaMemcpyHostToDevice));
+    // the solver's form: TMA-staged where keep <= 128, with its timeout flag
     bbjd_status s = restart_gemm(n, (int)k, (int)keep, reinterpret_cast<const cplx *>(X), ldx, dZ, (int)k,
-                                 reinterpret_cast<cplx *>(out), st);
-    if (!s && cudaStreamSynchronize(st) != cudaSuccess) s = BBJD_ERR_CUDA;
+                                 reinterpret_cast<cplx *>(out), st, derr);
+    int herr = 0;
+    if (!s && (cudaStreamSynchronize(st) != cudaSuccess ||
+               cudaMemcpy(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess))
+        s = BBJD_ERR_CUDA;
+    if (!s && herr) s = BBJD_ERR_DEVICE_TIMEOUT;
     cudaFree(dZ);
+    cudaFree(derr);
     return s;
 }
 

@@ -13,6 +13,9 @@
 // depend on scheduling.
 #include "dense.cuh"
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include <algorithm>
 #include <cstdio>
 #include <map>
@@ -237,8 +240,8 @@ __global__ void __launch_bounds__(256) k_update(
 constexpr int UD_TR = 32;          // rows per tile
 constexpr int UD_LD = UD_TR + 1;   // shared-memory stride of a tile column
 constexpr int UD_WARPS = 16;
-constexpr int UD_CPW = 14;         // phase-2 columns per warp: ncols <= 224
-constexpr int UD_HPL = 7;          // phase-1 columns per lane: ncols <= 224
+constexpr int UD_CPW = 14;         // phase-2 columns per warp (largest instance): ncols <= 224
+constexpr int UD_HPL = 7;          // phase-1 columns per lane (largest instance)
 constexpr int UD_MIN_COLS = 64;    // below, the separate dot pass is as cheap
 constexpr size_t UD_SMEM_LIMIT = 231424;
 
@@ -264,7 +267,7 @@ __device__ __forceinline__ void cp_async16(void *smem, const void *gmem, int src
                  : "memory");
 }
 
-template <int NST>
+template <int NST, int CPW>
 __global__ void __launch_bounds__(UD_WARPS * 32, 1) k_update_dot(
     int64_t n, int ncols, int64_t ld, const cplx *__restrict__ Q, const cplx *__restrict__ h1,
     const cplx *__restrict__ h2, cplx c1, cplx c2, cplx a, const cplx *v_in, cplx b,
@@ -279,9 +282,10 @@ __global__ void __launch_bounds__(UD_WARPS * 32, 1) k_update_dot(
     double *wn = reinterpret_cast<double *>(vs + UD_TR);   // per-warp ||v_out||^2
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     // phase-1 coefficients of this lane's columns
-    cplx hr[UD_HPL];
+    constexpr int HPL = CPW / 2;   // phase-1 columns per lane
+    cplx hr[HPL];
 #pragma unroll
-    for (int c = 0; c < UD_HPL; ++c) {
+    for (int c = 0; c < HPL; ++c) {
         const int j = lane + 32 * c;
         cplx h = mk(0.0, 0.0);
         if (j < ncols) {
@@ -291,14 +295,23 @@ __global__ void __launch_bounds__(UD_WARPS * 32, 1) k_update_dot(
         hr[c] = h;
     }
     const int64_t ntiles = (n + UD_TR - 1) / UD_TR;
+    // Thread tid copies element (tid & 31) of columns (tid >> 5) + 16 i,
+    // i = 0, 1, ...: its source and destination advance by fixed strides.
+    const int cr = tid & (UD_TR - 1), cj0 = tid >> 5;
+    const cplx *qsrc = Q + (int64_t)cj0 * ld + cr;
+    const int64_t qstep = (int64_t)UD_WARPS * ld;
+    const int dst0 = cj0 * UD_LD + cr;
     // rows past n are zero-filled (source size 0), so they add nothing
     auto issue = [&](int64_t tile, cplx *dst) {
         const int64_t row0 = tile * UD_TR;
-        for (int e = tid; e < ncols * UD_TR; e += blockDim.x) {
-            const int j = e >> 5, r = e & 31;
-            const int64_t row = row0 + r;
-            const bool in = row < n;
-            cp_async16(dst + j * UD_LD + r, Q + (int64_t)j * ld + (in ? row : 0), in ? 16 : 0);
+        const bool in = row0 + cr < n;
+        const cplx *src = qsrc + (in ? row0 : -cr);
+        const int bytes = in ? 16 : 0;
+        int d = dst0;
+        for (int j = cj0; j < ncols; j += UD_WARPS) {
+            cp_async16(dst + d, src, bytes);
+            src += qstep;
+            d += UD_WARPS * UD_LD;
         }
         if (tid < 2 * UD_TR) {
             const cplx *src = tid < UD_TR ? v_in : w_in;
@@ -310,9 +323,9 @@ __global__ void __launch_bounds__(UD_WARPS * 32, 1) k_update_dot(
             }
         }
     };
-    cplx acc[UD_CPW];
+    cplx acc[CPW];
 #pragma unroll
-    for (int c = 0; c < UD_CPW; ++c) acc[c] = mk(0.0, 0.0);
+    for (int c = 0; c < CPW; ++c) acc[c] = mk(0.0, 0.0);
     double nsq = 0.0;
     int buf = 0;
     int64_t tile = blockIdx.x;
@@ -343,7 +356,7 @@ __global__ void __launch_bounds__(UD_WARPS * 32, 1) k_update_dot(
             const int r = warp + UD_WARPS * q;
             cplx p = mk(0.0, 0.0);
 #pragma unroll
-            for (int c = 0; c < UD_HPL; ++c) {
+            for (int c = 0; c < HPL; ++c) {
                 const int j = lane + 32 * c;
                 if (j < ncols) cfma(p, Qt[j * UD_LD + r], hr[c]);
             }
@@ -366,7 +379,7 @@ __global__ void __launch_bounds__(UD_WARPS * 32, 1) k_update_dot(
         // phase 2: conj(Q) v_out for this warp's columns, lane = row
         const cplx vo = vs[lane];
 #pragma unroll
-        for (int c = 0; c < UD_CPW; ++c) {
+        for (int c = 0; c < CPW; ++c) {
             const int j = warp + UD_WARPS * c;
             if (j < ncols) cfmac(acc[c], Qt[j * UD_LD + lane], vo);
         }
@@ -375,7 +388,7 @@ __global__ void __launch_bounds__(UD_WARPS * 32, 1) k_update_dot(
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     cplx *out = partial + (int64_t)blockIdx.x * (ncols + 1);
 #pragma unroll
-    for (int c = 0; c < UD_CPW; ++c) {
+    for (int c = 0; c < CPW; ++c) {
         const int j = warp + UD_WARPS * c;
         const cplx sum = warp_sum(acc[c]);
         if (lane == 0 && j < ncols) out[j] = sum;
@@ -517,6 +530,139 @@ __global__ void __launch_bounds__(256) k_restart_gemm(int64_t n, int k, int keep
     }
 }
 
+// The same GEMM with its operands staged by the tensor-memory accelerator:
+// per 16-column K-slice, one 2D TMA load brings the CTA's 64 x 16 tile of X
+// (a box of 128 doubles x 16 columns over X viewed as a 2n x k FP64 array)
+// and one the 16 x 16 RC slice of Z, into a four-stage ring completed
+// through mbarrier transaction counts; thread 0 issues, three slices stay in
+// flight while one is multiplied.  Out-of-range rows and columns arrive as
+// zeros.  The FP64 FMA loop and the register tile are k_restart_gemm's.
+// Every mbarrier wait is bounded: a wait that runs out sets *err and the
+// CTA returns without writing (the caller reports a device timeout).
+__device__ __forceinline__ unsigned smem_u32(const void *p) {
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+// true once the barrier's phase `parity` has completed; false after
+// `limit` polls
+__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity, int limit) {
+    const unsigned a = smem_u32(bar);
+    for (int it = 0; it < limit; ++it) {
+        unsigned ok;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+            " selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(ok)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int x, int y,
+                                            unsigned long long *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3}], [%4];\n" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+
+constexpr int RT_STAGES = 4;
+constexpr int RT_WAIT_LIMIT = 1 << 22;
+template <int RC>
+constexpr size_t restart_tma_smem() {
+    // + 128: the ring starts at the first 128-byte boundary of the block
+    return sizeof(cplx) * (size_t)RT_STAGES * (RG_KS * RG_ROWS + 16 * RC * RG_KS) + 128;
+}
+
+template <int RC>
+__global__ void __launch_bounds__(256, 1) k_restart_gemm_tma(const __grid_constant__ CUtensorMap tx,
+                                                             const __grid_constant__ CUtensorMap tz,
+                                                             int64_t n, int k, int keep, int64_t ldx,
+                                                             cplx *out, int *err) {
+    constexpr int XT = RG_KS * RG_ROWS;     // X tile: [16 columns][64 rows]
+    constexpr int ZT = 16 * RC * RG_KS;     // Z slice: [16 RC columns][16 rows]
+    constexpr unsigned BYTES = (unsigned)(sizeof(cplx) * (XT + ZT));
+    extern __shared__ __align__(128) unsigned char rt_smem[];
+    // TMA destinations 128-byte aligned whatever the block's static layout
+    unsigned char *base = rt_smem + ((128u - (smem_u32(rt_smem) & 127u)) & 127u);
+    cplx *sx = reinterpret_cast<cplx *>(base);
+    cplx *sz = sx + RT_STAGES * XT;
+    __shared__ __align__(8) unsigned long long full[RT_STAGES];
+    __shared__ int abort_flag;
+    const int tid = threadIdx.x, rg = tid & 15, cg = tid >> 4;
+    const int64_t row0 = (int64_t)blockIdx.x * RG_ROWS;
+    const int nk = (k + RG_KS - 1) / RG_KS;
+    if (tid == 0) {
+        for (int st = 0; st < RT_STAGES; ++st) mbar_init(&full[st], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        abort_flag = 0;
+    }
+    __syncthreads();
+    auto load = [&](int kt) {
+        const int st = kt % RT_STAGES;
+        mbar_expect_tx(&full[st], BYTES);
+        tma_load_2d(sx + st * XT, &tx, (int)(2 * row0), kt * RG_KS, &full[st]);
+        tma_load_2d(sz + st * ZT, &tz, kt * 2 * RG_KS, 0, &full[st]);
+    };
+    if (tid == 0)
+        for (int kt = 0; kt < RT_STAGES - 1 && kt < nk; ++kt) load(kt);
+    cplx acc[4][RC];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < RC; ++v) acc[u][v] = mk(0.0, 0.0);
+    for (int kt = 0; kt < nk; ++kt) {
+        const int st = kt % RT_STAGES;
+        // the stage of slice kt - 1 was released by the barrier that ended it
+        if (tid == 0 && kt + RT_STAGES - 1 < nk) load(kt + RT_STAGES - 1);
+        if (!mbar_wait(&full[st], (unsigned)((kt / RT_STAGES) & 1), RT_WAIT_LIMIT)) abort_flag = 1;
+        const cplx *X = sx + st * XT, *Z = sz + st * ZT;
+#pragma unroll 4
+        for (int jj = 0; jj < RG_KS; ++jj) {
+            cplx xv[4], zv[RC];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) xv[u] = X[jj * RG_ROWS + rg + 16 * u];
+#pragma unroll
+            for (int v = 0; v < RC; ++v) zv[v] = Z[(cg + 16 * v) * RG_KS + jj];
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int v = 0; v < RC; ++v) cfma(acc[u][v], xv[u], zv[v]);
+        }
+        __syncthreads();
+        if (abort_flag) {
+            if (tid == 0) {
+                atomicExch(err, 1);
+                // wait (bounded) for the slices still in flight before leaving
+                const int issued = min(nk, kt + RT_STAGES);
+                for (int q = kt; q < issued; ++q)
+                    mbar_wait(&full[q % RT_STAGES], (unsigned)((q / RT_STAGES) & 1), RT_WAIT_LIMIT);
+            }
+            return;
+        }
+    }
+    // every CTA reads only its own 64 rows of X, so out may alias X
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const int64_t row = row0 + rg + 16 * u;
+        if (row >= n) continue;
+#pragma unroll
+        for (int v = 0; v < RC; ++v) {
+            const int col = cg + 16 * v;
+            if (col < keep) out[(int64_t)col * ldx + row] = acc[u][v];
+        }
+    }
+}
+
 // Gram stage 1: partial[g] (keep x keep, column-major) = X_g^H Y_g over the
 // CTA's row range.  Each thread holds a 5 x 5 tile (keep <= 80 per launch
 // tile; larger keep tiles over blockIdx.y / z).
@@ -633,8 +779,11 @@ bbjd_status Scratch::init(int64_t n_, int max_cols, int nvec) {
     BBJD_CUDA_TRY(cudaMemset(flags, 0, sizeof(int) * 16));
     // the fused CGS update stages tiles of the basis in up to 226 KB
     bbjd_status s;
-    if ((s = raise_smem_limit((const void *)k_update_dot<2>, UD_SMEM_LIMIT))) return s;
-    if ((s = raise_smem_limit((const void *)k_update_dot<3>, UD_SMEM_LIMIT))) return s;
+    for (const void *f : {(const void *)k_update_dot<3, 4>, (const void *)k_update_dot<3, 6>,
+                          (const void *)k_update_dot<3, 8>, (const void *)k_update_dot<3, 10>,
+                          (const void *)k_update_dot<2, 10>, (const void *)k_update_dot<2, 12>,
+                          (const void *)k_update_dot<2, 14>})
+        if ((s = raise_smem_limit(f, UD_SMEM_LIMIT))) return s;
     const size_t smem_need = sizeof(cplx) * 2 * (size_t)rpc;
     if ((s = raise_smem_limit((const void *)k_tsdot<1, 2>, smem_need))) return s;
     if ((s = raise_smem_limit((const void *)k_tsdot<2, 1>, smem_need))) return s;
@@ -698,14 +847,24 @@ bbjd_status cgs_tail(Scratch &S, int ncols, int64_t ld, const cplx *Q, const cpl
         const int64_t ntiles = (S.n + UD_TR - 1) / UD_TR;
         const int G = (int)std::max<int64_t>(1, std::min<int64_t>({(int64_t)num_sms(), ntiles,
                                                                     (int64_t)S.G}));
-        if (update_dot_stages(ncols) == 3)
-            k_update_dot<3><<<G, UD_WARPS * 32, update_dot_smem(ncols, 3), st>>>(
-                S.n, ncols, ld, Q, h1, h2, c1, c2, a, v_in, b, w_in, v_out, S.partial, S.nrm_part,
-                S.counter, norm_out, ref_nsq, ref_nrm, flag);
-        else
-            k_update_dot<2><<<G, UD_WARPS * 32, update_dot_smem(ncols, 2), st>>>(
-                S.n, ncols, ld, Q, h1, h2, c1, c2, a, v_in, b, w_in, v_out, S.partial, S.nrm_part,
-                S.counter, norm_out, ref_nsq, ref_nrm, flag);
+        const int nst = update_dot_stages(ncols);
+        // the narrowest instance that covers ncols: 16 CPW columns
+        const int cpw = std::max(4, ((ncols + 15) / 16 + 1) / 2 * 2);
+#define BBJD_UD(NST, CPW)                                                                         \
+    k_update_dot<NST, CPW><<<G, UD_WARPS * 32, update_dot_smem(ncols, NST), st>>>(                \
+        S.n, ncols, ld, Q, h1, h2, c1, c2, a, v_in, b, w_in, v_out, S.partial, S.nrm_part, S.counter, \
+        norm_out, ref_nsq, ref_nrm, flag)
+        if (nst == 3) {
+            if (cpw <= 4) BBJD_UD(3, 4);
+            else if (cpw <= 6) BBJD_UD(3, 6);
+            else if (cpw <= 8) BBJD_UD(3, 8);
+            else BBJD_UD(3, 10);
+        } else {
+            if (cpw <= 10) BBJD_UD(2, 10);
+            else if (cpw <= 12) BBJD_UD(2, 12);
+            else BBJD_UD(2, 14);
+        }
+#undef BBJD_UD
         BBJD_LAUNCH_CHECK();
         k_reduce<<<(ncols + 1 + 31) / 32, 256, 0, st>>>(S.partial, G, ncols + 1, h_re, flag);
         BBJD_LAUNCH_CHECK();
@@ -749,8 +908,65 @@ bbjd_status svdv(Scratch &S, const cplx *dots, const cplx *z, const cplx *s, cpl
     return BBJD_SUCCESS;
 }
 
+// cuTensorMapEncodeTiled from the driver, through the runtime (no link
+// against libcuda); null when the driver does not provide it.
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+// A 2D FP64 tensor map: d0 contiguous doubles per column, d1 columns
+// stride_bytes apart, boxes of b0 x b1, zeros outside.
+static bool fp64_map(CUtensorMap *m, const void *base, uint64_t d0, uint64_t d1, uint64_t stride_bytes,
+                     uint32_t b0, uint32_t b1) {
+    const auto fn = tensor_map_encoder();
+    if (!fn || ((uintptr_t)base & 15) || (stride_bytes & 15)) return false;
+    cuuint64_t dims[2] = {d0, d1};
+    cuuint64_t strides[1] = {stride_bytes};
+    cuuint32_t box[2] = {b0, b1};
+    cuuint32_t es[2] = {1, 1};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<void *>(base), dims, strides, box, es,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <int RC>
+static bool restart_gemm_tma(int64_t n, int k, int keep, const cplx *X, int64_t ldx, const cplx *Z_dev,
+                             int ldz, cplx *out, int *err, cudaStream_t st) {
+    CUtensorMap tx, tz;
+    // X as a 2n x k FP64 array (real and imaginary parts interleaved); its
+    // tile origin x = 2 row0 is a multiple of 128 doubles, so 16-byte aligned
+    if (!fp64_map(&tx, X, 2 * (uint64_t)n, (uint64_t)k, 16 * (uint64_t)ldx, 2 * RG_ROWS, RG_KS)) return false;
+    if (!fp64_map(&tz, Z_dev, 2 * (uint64_t)k, (uint64_t)keep, 16 * (uint64_t)ldz, 2 * RG_KS, 16 * RC))
+        return false;
+    if (raise_smem_limit((const void *)k_restart_gemm_tma<RC>, restart_tma_smem<RC>())) return false;
+    const unsigned gx = (unsigned)((n + RG_ROWS - 1) / RG_ROWS);
+    k_restart_gemm_tma<RC><<<gx, 256, restart_tma_smem<RC>(), st>>>(tx, tz, n, k, keep, ldx, out, err);
+    return true;
+}
+
 bbjd_status restart_gemm(int64_t n, int k, int keep, const cplx *X, int64_t ldx, const cplx *Z_dev,
-                         int ldz, cplx *out, cudaStream_t st) {
+                         int ldz, cplx *out, cudaStream_t st, int *err) {
+    // TMA-staged form (one column tile, keep <= 128) when the caller takes a
+    // timeout flag; the plain form otherwise
+    if (err && k > 0 && keep > 0 && keep <= 16 * 8) {
+        bool ok = keep <= 16 * 2   ? restart_gemm_tma<2>(n, k, keep, X, ldx, Z_dev, ldz, out, err, st)
+                  : keep <= 16 * 5 ? restart_gemm_tma<5>(n, k, keep, X, ldx, Z_dev, ldz, out, err, st)
+                                   : restart_gemm_tma<8>(n, k, keep, X, ldx, Z_dev, ldz, out, err, st);
+        if (ok) {
+            BBJD_LAUNCH_CHECK();
+            return BBJD_SUCCESS;
+        }
+    }
     const unsigned gx = (unsigned)((n + RG_ROWS - 1) / RG_ROWS);
     // one column tile covers keep <= 16*RC; in-place needs a single tile
     if (keep <= 16 * 2) {

@@ -59,8 +59,11 @@ bbjd_status axpby_n(int64_t count, cplx a, const cplx *x, cplx b, const cplx *y,
                     cudaStream_t st);
 bbjd_status svdv(Scratch &S, const cplx *dots, const cplx *z, const cplx *s, cplx *out,
                  cudaStream_t st);
+// out (n x keep) = X (n x k) Z (k x keep); out may alias X.  With err (a
+// device int) the operands are staged by TMA and a bounded wait that runs
+// out sets *err to 1 (nothing is written then).
 bbjd_status restart_gemm(int64_t n, int k, int keep, const cplx *X, int64_t ldx, const cplx *Z_dev,
-                         int ldz, cplx *out, cudaStream_t st);
+                         int ldz, cplx *out, cudaStream_t st, int *err = nullptr);
 // Raise the dynamic shared-memory limit of the one-matrix, one-vector dot
 // kernel to `bytes` (no-op up to 48 KB).
 bbjd_status tsdot_allow_smem(size_t bytes);

@@ -117,7 +117,7 @@ static inline zc Z(cplx c) { return zc(c.x, c.y); }
 // device scalar slots
 enum { SC_UNORM = 0, SC_RNORM, SC_VNORM, SC_WNORM, SC_TMP, SC_TMP2, SC_GNORM, SC_WPRE, SC_N };
 // device flag slots
-enum { FL_V = 0, FL_W, FL_T, FL_G, FL_N };
+enum { FL_V = 0, FL_W, FL_T, FL_G, FL_TMO, FL_N };
 
 // ---------------------------------------------------------------------------
 cudaEvent_t Timer::get() {
@@ -1493,7 +1493,7 @@ int Engine::rebuild_W_cholqr(int keep) {
             for (int i = 0; i < keep; ++i) g[i + (size_t)j * keep] = i <= j ? C(R[i + (size_t)j * keep]) : mk(0, 0);
         if (cudaMemcpyAsync(Zdev, g.data(), sizeof(cplx) * keep * keep, cudaMemcpyHostToDevice, st)) return -1;
         T.begin(KC_RESTART, 32.0 * n * keep);
-        if (restart_gemm(n, keep, keep, W, ld, Zdev, keep, W, st)) return -1;
+        if (restart_gemm(n, keep, keep, W, ld, Zdev, keep, W, st, dflag + FL_TMO)) return -1;
         T.end();
         bytes_dev += 32.0 * n * keep;
         if (sync()) return -1;      // g is reused by the next pass
@@ -1748,10 +1748,11 @@ bbjd_status Engine::run() {
             }
             const double gb = 16.0 * n * (double)(k + keep);
             T.begin(KC_RESTART, 3 * gb);
-            if ((s = restart_gemm(n, (int)k, (int)keep, V, ld, Zdev, (int)k, V, st))) return s;
+            int *tmo = dflag + FL_TMO;
+            if ((s = restart_gemm(n, (int)k, (int)keep, V, ld, Zdev, (int)k, V, st, tmo))) return s;
             if (mixed && (s = to_c64(n * keep, V, Vs, st))) return s;
-            if ((s = restart_gemm(n, (int)k, (int)keep, AV, ld, Zdev, (int)k, AV, st))) return s;
-            if ((s = restart_gemm(n, (int)k, (int)keep, BV, ld, Zdev, (int)k, BV, st))) return s;
+            if ((s = restart_gemm(n, (int)k, (int)keep, AV, ld, Zdev, (int)k, AV, st, tmo))) return s;
+            if ((s = restart_gemm(n, (int)k, (int)keep, BV, ld, Zdev, (int)k, BV, st, tmo))) return s;
             T.end();
             bytes_dev += 3 * gb;
             // rebuild W from the kept test images (jd_core.c:1002-1010): the
@@ -1781,7 +1782,11 @@ bbjd_status Engine::run() {
                 std::vector<cplx> gh((size_t)2 * keep * keep);
                 BBJD_CUDA_TRY(cudaMemcpyAsync(gh.data(), gram_out, sizeof(cplx) * 2 * keep * keep,
                                               cudaMemcpyDeviceToHost, st));
+                BBJD_CUDA_TRY(cudaMemcpyAsync(pin_i + FL_TMO, dflag + FL_TMO, sizeof(int),
+                                              cudaMemcpyDeviceToHost, st));
                 if ((s = sync())) return s;
+                // a TMA-staged restart GEMM whose bounded wait ran out
+                if (pin_i[FL_TMO]) return res->status = BBJD_ERR_DEVICE_TIMEOUT;
                 for (int64_t c = 0; c < keep; ++c)
                     for (int64_t i = 0; i < keep; ++i) {
                         ws->MA[i + (size_t)c * maxsub] = Z(gh[c * keep + i]);

@@ -19,7 +19,10 @@ pencil and its LU already in HBM (CUDA events around the call, max over
 ranks); `e2e` = the same through the public API from pinned host buffers:
 upload of the pencil, device LU factorisation, the solve, and the copy of
 the eigenvectors back to the host, all inside the timed region.  Inputs are
-larger than L2 (4.1 GB pencil), so no flush is needed.
+larger than L2 (4.1 GB pencil), so no flush is needed.  `detail` also
+times a window of outer iterations of the inner-GMRES configuration on the
+same pencil (k = 32, maxsub 120, minsub 48, block-Jacobi preconditioner,
+GMRES 50 steps to 1e-3) in both forms.
 
 Multi-GPU (torchrun, one process per GPU): rank r solves its own pencil of
 the sigma-sweep (generator seed r); nothing is exchanged (weak scaling).
@@ -300,6 +303,36 @@ def _compare_forms(ev_a, ev_b):
     return d, same
 
 
+GMRES_CONFIG = dict(k=32, maxsub=120, minsub=48, inner_maxiter=50, inner_tol=1e-3)
+
+
+def gmres_window(dev, v0, iters, form, timed):
+    """The inner-GMRES configuration on the same pencil: block-Jacobi
+    preconditioner (b x b diagonal-block LU of A - sigma B), left-
+    preconditioned GMRES of at most 50 steps to 1e-3 with the projectors in
+    FP64 (complex64 Arnoldi basis in the mixed form), k = 32, maxsub 120,
+    minsub 48, for a fixed window of outer iterations (a full solve to 32
+    pairs takes thousands): seconds per outer iteration, pairs converged in
+    the window, and the device classes."""
+    from bbjd_b200 import DevicePreconditioner, jdqz
+    w = WORKLOAD
+    pc = DevicePreconditioner(dev, w["sigma"], "block_jacobi", precision=form)
+    kw = dict(sigma=w["sigma"], tol=w["tol"], maxiter=iters, v0=v0, return_info=True,
+              precision=form, **GMRES_CONFIG)
+    jdqz(dev, preconditioner=pc, timing=False, **dict(kw, maxiter=3))      # warm-up
+    dt, out = timed(lambda: jdqz(dev, preconditioner=pc, timing=True, **kw))
+    pc.close()
+    info = out[2]
+    d = info["device"]
+    return {"form": form, "outer_iters": info["iters"], "seconds": round(dt, 3),
+            "s_per_iter": round(dt / max(info["iters"], 1), 4), "nconv": info["nconv"],
+            "seconds_device_timed": round(d["seconds_device"], 3),
+            "seconds_qz_host": round(d["seconds_qz"], 3),
+            "kernels": {k: {"ms": round(v["ms"], 1),
+                            "GBps": round(v["bytes"] / max(v["ms"], 1e-9) / 1e6, 1)}
+                        for k, v in d["kernels"].items() if v["calls"]}}
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -380,6 +413,9 @@ def run_ours(args):
             return r
         e2e.append(timed(full))
 
+    gmres = [gmres_window(dev, v0, args.gmres_iters, f, timed) for f in forms] \
+        if args.gmres_iters > 0 else []
+
     # max over ranks of the seconds, sum of the pairs
     secs = [sum(r[0] for r in timed_res[f]) for f in forms] + [sum(r[0] for r in e2e)]
     pairs = [sum(r[1][2]["nconv"] for r in timed_res[f]) for f in forms] + \
@@ -436,6 +472,10 @@ def run_ours(args):
             "eigenvalue_distance_to_nearest_in_other": [float(f"{x:.3e}") for x in dist_h],
             "max_distance_same_eigenvalue": max([x for x, lam in zip(dist_h, ev_h)
                                                  if x <= 1e-8 * max(1.0, abs(lam))], default=None)}
+    if gmres:
+        detail["gmres_block_jacobi"] = {"config": {"workload": WORKLOAD_NAME, **GMRES_CONFIG,
+                                                   "preconditioner": "block Jacobi (device)"},
+                                        "forms": gmres}
     line = {
         "metric": "eigenpairs/s", "value": hs["value"], "unit": "eigenpairs/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -492,6 +532,9 @@ def main():
                          "while the device iterates on the guessed target; off: serially")
     ap.add_argument("--ref-iters", type=int, default=16,
                     help="reference outer iterations per CPU sample step")
+    ap.add_argument("--gmres-iters", type=int, default=100,
+                    help="outer iterations of the inner-GMRES configuration reported in detail "
+                         "(0: skip)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":

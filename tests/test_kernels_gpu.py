@@ -147,7 +147,10 @@ def test_orthogonalize_matches_oracle(n, k, repass):
         assert np.abs(Q.conj().T @ _host(vd)).max() < 1e-12 * np.linalg.norm(v)
 
 
-@pytest.mark.parametrize("n,k,keep", [(1000, 40, 20), (100000, 200, 80), (777, 30, 29), (5000, 150, 128)])
+# keep <= 128: the TMA-staged kernel (in place); 64-row tiles and 16-column
+# K-slices with ragged ends, one- and three-column-tile widths
+@pytest.mark.parametrize("n,k,keep", [(1000, 40, 20), (100000, 200, 80), (777, 30, 29), (5000, 150, 128),
+                                      (64, 17, 16), (130, 1, 1), (4159, 200, 128), (20000, 97, 33)])
 def test_restart_gemm_matches_numpy(n, k, keep):
     import torch
     rng = np.random.default_rng(1)
