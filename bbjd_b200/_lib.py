@@ -119,6 +119,8 @@ SIGNATURES = {
                                                 C.POINTER(C.c_int), C.c_void_p]),
     "bbjd_dev_restart_gemm": (C.c_int, [bbjd_int, bbjd_int, bbjd_int, C.c_void_p, bbjd_int,
                                         C.c_void_p, bbjd_int, C.c_void_p, C.c_void_p]),
+    "bbjd_dev_restart_gemm_stalled": (C.c_int, [bbjd_int, bbjd_int, bbjd_int, C.c_void_p, bbjd_int,
+                                        C.c_void_p, bbjd_int, C.c_void_p, C.c_void_p]),
     "bbjd_dev_gram": (C.c_int, [bbjd_int, bbjd_int, C.c_void_p, C.c_void_p, bbjd_int,
                                 C.c_void_p, bbjd_int, C.c_void_p]),
     "bbjd_gpu_version": (C.c_char_p, []),

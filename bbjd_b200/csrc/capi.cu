@@ -465,9 +465,9 @@ bbjd_status bbjd_dev_orthogonalize(bbjd_int n, bbjd_int k, const bbjd_zomplex *Q
     return s;
 }
 
-bbjd_status bbjd_dev_restart_gemm(bbjd_int n, bbjd_int k, bbjd_int keep, const bbjd_zomplex *X,
-                                  bbjd_int ldx, const bbjd_zomplex *Z_host, bbjd_int ldz,
-                                  bbjd_zomplex *out, void *stream) {
+static bbjd_status dev_restart_gemm(bbjd_int n, bbjd_int k, bbjd_int keep, const bbjd_zomplex *X,
+                                    bbjd_int ldx, const bbjd_zomplex *Z_host, bbjd_int ldz,
+                                    bbjd_zomplex *out, void *stream, bool stalled) {
     if (n < 1 || k < 1 || keep < 1 || !X || !Z_host || !out || ldz < k || ldx < n) return BBJD_ERR_INVALID;
     cudaStream_t st = (cudaStream_t)stream;
     cplx *dZ = nullptr;
@@ -480,8 +480,10 @@ bbjd_status bbjd_dev_restart_gemm(bbjd_int n, bbjd_int k, bbjd_int keep, const b
     BBJD_CUDA_TRY(cudaMemset(derr, 0, sizeof(int)));
     BBJD_CUDA_TRY(cudaMemcpy(dZ, zh.data(), sizeof(cplx) * zh.size(), cudaMemcpyHostToDevice));
     // the solver's form: TMA-staged where keep <= 128, with its timeout flag
-    bbjd_status s = restart_gemm(n, (int)k, (int)keep, reinterpret_cast<const cplx *>(X), ldx, dZ, (int)k,
-                                 reinterpret_cast<cplx *>(out), st, derr);
+    bbjd_status s = stalled ? restart_gemm_stalled(n, (int)k, (int)keep, reinterpret_cast<const cplx *>(X),
+                                                   ldx, dZ, (int)k, reinterpret_cast<cplx *>(out), st, derr)
+                            : restart_gemm(n, (int)k, (int)keep, reinterpret_cast<const cplx *>(X), ldx, dZ,
+                                           (int)k, reinterpret_cast<cplx *>(out), st, derr);
     int herr = 0;
     if (!s && (cudaStreamSynchronize(st) != cudaSuccess ||
                cudaMemcpy(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess))
@@ -490,6 +492,19 @@ bbjd_status bbjd_dev_restart_gemm(bbjd_int n, bbjd_int k, bbjd_int keep, const b
     cudaFree(dZ);
     cudaFree(derr);
     return s;
+}
+
+bbjd_status bbjd_dev_restart_gemm(bbjd_int n, bbjd_int k, bbjd_int keep, const bbjd_zomplex *X,
+                                  bbjd_int ldx, const bbjd_zomplex *Z_host, bbjd_int ldz,
+                                  bbjd_zomplex *out, void *stream) {
+    return dev_restart_gemm(n, k, keep, X, ldx, Z_host, ldz, out, stream, false);
+}
+
+bbjd_status bbjd_dev_restart_gemm_stalled(bbjd_int n, bbjd_int k, bbjd_int keep, const bbjd_zomplex *X,
+                                          bbjd_int ldx, const bbjd_zomplex *Z_host, bbjd_int ldz,
+                                          bbjd_zomplex *out, void *stream) {
+    if (keep > 80) return BBJD_ERR_INVALID;
+    return dev_restart_gemm(n, k, keep, X, ldx, Z_host, ldz, out, stream, true);
 }
 
 bbjd_status bbjd_dev_gram(bbjd_int n, bbjd_int keep, const bbjd_zomplex *X, const bbjd_zomplex *Y,

@@ -550,11 +550,12 @@ __device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned
                  "r"(bytes)
                  : "memory");
 }
-// true once the barrier's phase `parity` has completed; false after
-// `limit` polls
-__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity, int limit) {
+// true once the barrier's phase `parity` has completed; false when that
+// has not happened within `max_cycles` SM clock cycles
+__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity, long long max_cycles) {
     const unsigned a = smem_u32(bar);
-    for (int it = 0; it < limit; ++it) {
+    const long long t0 = clock64();
+    for (;;) {
         unsigned ok;
         asm volatile(
             "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
@@ -563,8 +564,8 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned pari
             : "r"(a), "r"(parity)
             : "memory");
         if (ok) return true;
+        if (clock64() - t0 > max_cycles) return false;
     }
-    return false;
 }
 __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int x, int y,
                                             unsigned long long *bar) {
@@ -576,7 +577,8 @@ __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, i
 }
 
 constexpr int RT_STAGES = 4;
-constexpr int RT_WAIT_LIMIT = 1 << 22;
+// a stage that has not landed after ~1 s (2e9 cycles at <= 2 GHz) never will
+constexpr long long RT_WAIT_CYCLES = 2000000000LL;
 template <int RC>
 constexpr size_t restart_tma_smem() {
     // + 128: the ring starts at the first 128-byte boundary of the block
@@ -587,7 +589,8 @@ template <int RC>
 __global__ void __launch_bounds__(256, 1) k_restart_gemm_tma(const __grid_constant__ CUtensorMap tx,
                                                              const __grid_constant__ CUtensorMap tz,
                                                              int64_t n, int k, int keep, int64_t ldx,
-                                                             cplx *out, int *err) {
+                                                             cplx *out, int *err, long long wait_cycles,
+                                                             unsigned tx_extra) {
     constexpr int XT = RG_KS * RG_ROWS;     // X tile: [16 columns][64 rows]
     constexpr int ZT = 16 * RC * RG_KS;     // Z slice: [16 RC columns][16 rows]
     constexpr unsigned BYTES = (unsigned)(sizeof(cplx) * (XT + ZT));
@@ -609,7 +612,7 @@ __global__ void __launch_bounds__(256, 1) k_restart_gemm_tma(const __grid_consta
     __syncthreads();
     auto load = [&](int kt) {
         const int st = kt % RT_STAGES;
-        mbar_expect_tx(&full[st], BYTES);
+        mbar_expect_tx(&full[st], BYTES + tx_extra);
         tma_load_2d(sx + st * XT, &tx, (int)(2 * row0), kt * RG_KS, &full[st]);
         tma_load_2d(sz + st * ZT, &tz, kt * 2 * RG_KS, 0, &full[st]);
     };
@@ -624,7 +627,7 @@ __global__ void __launch_bounds__(256, 1) k_restart_gemm_tma(const __grid_consta
         const int st = kt % RT_STAGES;
         // the stage of slice kt - 1 was released by the barrier that ended it
         if (tid == 0 && kt + RT_STAGES - 1 < nk) load(kt + RT_STAGES - 1);
-        if (!mbar_wait(&full[st], (unsigned)((kt / RT_STAGES) & 1), RT_WAIT_LIMIT)) abort_flag = 1;
+        if (!mbar_wait(&full[st], (unsigned)((kt / RT_STAGES) & 1), wait_cycles)) abort_flag = 1;
         const cplx *X = sx + st * XT, *Z = sz + st * ZT;
 #pragma unroll 4
         for (int jj = 0; jj < RG_KS; ++jj) {
@@ -645,7 +648,7 @@ __global__ void __launch_bounds__(256, 1) k_restart_gemm_tma(const __grid_consta
                 // wait (bounded) for the slices still in flight before leaving
                 const int issued = min(nk, kt + RT_STAGES);
                 for (int q = kt; q < issued; ++q)
-                    mbar_wait(&full[q % RT_STAGES], (unsigned)((q / RT_STAGES) & 1), RT_WAIT_LIMIT);
+                    mbar_wait(&full[q % RT_STAGES], (unsigned)((q / RT_STAGES) & 1), wait_cycles);
             }
             return;
         }
@@ -941,7 +944,8 @@ static bool fp64_map(CUtensorMap *m, const void *base, uint64_t d0, uint64_t d1,
 
 template <int RC>
 static bool restart_gemm_tma(int64_t n, int k, int keep, const cplx *X, int64_t ldx, const cplx *Z_dev,
-                             int ldz, cplx *out, int *err, cudaStream_t st) {
+                             int ldz, cplx *out, int *err, cudaStream_t st,
+                             long long wait_cycles = RT_WAIT_CYCLES, unsigned tx_extra = 0) {
     CUtensorMap tx, tz;
     // X as a 2n x k FP64 array (real and imaginary parts interleaved); its
     // tile origin x = 2 row0 is a multiple of 128 doubles, so 16-byte aligned
@@ -950,8 +954,19 @@ static bool restart_gemm_tma(int64_t n, int k, int keep, const cplx *X, int64_t 
         return false;
     if (raise_smem_limit((const void *)k_restart_gemm_tma<RC>, restart_tma_smem<RC>())) return false;
     const unsigned gx = (unsigned)((n + RG_ROWS - 1) / RG_ROWS);
-    k_restart_gemm_tma<RC><<<gx, 256, restart_tma_smem<RC>(), st>>>(tx, tz, n, k, keep, ldx, out, err);
+    k_restart_gemm_tma<RC><<<gx, 256, restart_tma_smem<RC>(), st>>>(tx, tz, n, k, keep, ldx, out, err,
+                                                                    wait_cycles, tx_extra);
     return true;
+}
+
+bbjd_status restart_gemm_stalled(int64_t n, int k, int keep, const cplx *X, int64_t ldx,
+                                 const cplx *Z_dev, int ldz, cplx *out, cudaStream_t st, int *err) {
+    // every stage expects 16 bytes more than its two loads bring, so no
+    // stage ever completes; each wait gives up after ~1 ms
+    if (keep > 16 * 5 || !restart_gemm_tma<5>(n, k, keep, X, ldx, Z_dev, ldz, out, err, st, 2000000LL, 16u))
+        return BBJD_ERR_INVALID;
+    BBJD_LAUNCH_CHECK();
+    return BBJD_SUCCESS;
 }
 
 bbjd_status restart_gemm(int64_t n, int k, int keep, const cplx *X, int64_t ldx, const cplx *Z_dev,

@@ -64,6 +64,10 @@ bbjd_status svdv(Scratch &S, const cplx *dots, const cplx *z, const cplx *s, cpl
 // out sets *err to 1 (nothing is written then).
 bbjd_status restart_gemm(int64_t n, int k, int keep, const cplx *X, int64_t ldx, const cplx *Z_dev,
                          int ldz, cplx *out, cudaStream_t st, int *err = nullptr);
+// The TMA-staged form with a transaction count that never completes (the
+// failure-detection test): its bounded waits run out and set *err.
+bbjd_status restart_gemm_stalled(int64_t n, int k, int keep, const cplx *X, int64_t ldx,
+                                 const cplx *Z_dev, int ldz, cplx *out, cudaStream_t st, int *err);
 // Raise the dynamic shared-memory limit of the one-matrix, one-vector dot
 // kernel to `bytes` (no-op up to 48 KB).
 bbjd_status tsdot_allow_smem(size_t bytes);

@@ -224,6 +224,17 @@ bbjd_status bbjd_dev_restart_gemm(bbjd_int n, bbjd_int k, bbjd_int keep,
                                   const bbjd_zomplex *Z_host, bbjd_int ldz,
                                   bbjd_zomplex *out, void *stream);
 
+/* Failure-detection check of the restart GEMM's bounded waits (no
+ * counterpart in the reference): the same TMA-staged kernel, with every
+ * stage's mbarrier expecting 16 bytes more than its loads bring, so no
+ * stage completes; each wait gives up after ~1 ms and the call returns
+ * BBJD_ERR_DEVICE_TIMEOUT with out unchanged and the context usable.
+ * keep <= 80. */
+bbjd_status bbjd_dev_restart_gemm_stalled(bbjd_int n, bbjd_int k, bbjd_int keep,
+                                          const bbjd_zomplex *X, bbjd_int ldx,
+                                          const bbjd_zomplex *Z_host, bbjd_int ldz,
+                                          bbjd_zomplex *out, void *stream);
+
 /* C (host, keep x keep, ldc) = X^H Y for device X, Y (n x keep, ld = ldx).
  * reference jd_core.c:1020-1025 */
 bbjd_status bbjd_dev_gram(bbjd_int n, bbjd_int keep, const bbjd_zomplex *X,

@@ -6,7 +6,9 @@ a RuntimeError in Python), the status the reference maps a breakdown to
 (reference include/bbjd.h:70-78, bbjd.py:248-257), instead of iterating on
 non-finite numbers until maxiter.  A callback that fails returns
 BBJD_ERR_CALLBACK, and a Python exception inside a callback propagates
-unchanged (reference _bbjd_c.c:212-216)."""
+unchanged (reference _bbjd_c.c:212-216).  A device-side wait that runs out
+(the TMA-staged restart GEMM's mbarrier waits, made to wait for bytes that
+never come) returns BBJD_ERR_DEVICE_TIMEOUT and leaves the context usable."""
 import numpy as np
 import pytest
 import scipy.sparse as sp
@@ -98,3 +100,29 @@ def test_failing_callback_status_and_python_exception():
                  preconditioner=lu, v0=start_vector(P.n, 1))
     assert len(ev) == 2
     assert sp.issparse(A)
+
+
+def test_restart_gemm_wait_that_runs_out_is_a_device_timeout():
+    """Every stage of the stalled variant expects 16 bytes more than its TMA
+    loads bring, so no wait completes: each gives up after ~1 ms, the kernel
+    writes nothing and reports a timeout.  The same GEMM right after runs
+    normally on the same context."""
+    import torch
+
+    from bbjd_b200 import _lib
+    lib = _lib.load()
+    n, k, keep = 1000, 40, 20
+    rng = np.random.default_rng(2)
+    X = rng.standard_normal((n, k)) + 1j * rng.standard_normal((n, k))
+    Z = np.asfortranarray(rng.standard_normal((k, keep)) + 1j * rng.standard_normal((k, keep)))
+    Xd = torch.from_numpy(np.ascontiguousarray(X.T)).to("cuda")     # column-major n x k
+    before = Xd.clone()
+    st = lib.bbjd_dev_restart_gemm_stalled(n, k, keep, Xd.data_ptr(), n, Z.ctypes.data, k,
+                                           Xd.data_ptr(), None)
+    assert st == -7                                     # BBJD_ERR_DEVICE_TIMEOUT
+    assert torch.equal(Xd, before)                      # nothing written
+    assert lib.bbjd_dev_restart_gemm(n, k, keep, Xd.data_ptr(), n, Z.ctypes.data, k,
+                                     Xd.data_ptr(), None) == 0
+    out = Xd.cpu().numpy().reshape(-1, n).T[:, :keep]
+    ref = X @ Z
+    assert np.abs(out - ref).max() < 1e-12 * np.abs(ref).max()
