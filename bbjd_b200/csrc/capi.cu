@@ -455,10 +455,13 @@ bbjd_status bbjd_dev_orthogonalize(bbjd_int n, bbjd_int k, const bbjd_zomplex *Q
                              nullptr, dv, S.scal, S.red + k, nullptr, S.flags, S.red + S.maxX, st);
     }
     double nrm = 0.0;
-    int flag = 0;
+    int flag = 0, tmo = 0;
     if (!s && cudaMemcpyAsync(&nrm, S.scal, sizeof(double), cudaMemcpyDeviceToHost, st) != cudaSuccess) s = BBJD_ERR_CUDA;
     if (!s && k > 0 && cudaMemcpyAsync(&flag, S.flags, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess) s = BBJD_ERR_CUDA;
+    if (!s && cudaMemcpyAsync(&tmo, S.flags + SCRATCH_FLAG_TMO, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess)
+        s = BBJD_ERR_CUDA;
     if (!s && cudaStreamSynchronize(st) != cudaSuccess) s = BBJD_ERR_CUDA;
+    if (!s && tmo) s = BBJD_ERR_DEVICE_TIMEOUT;
     S.release();
     if (norm_out) *norm_out = nrm;
     if (second_pass_out) *second_pass_out = flag;

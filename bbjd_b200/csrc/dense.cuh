@@ -7,6 +7,10 @@ namespace bbjd {
 
 const char *last_error();
 
+// Device flag set (never cleared within a solve) by a kernel whose bounded
+// mbarrier wait ran out.
+constexpr int SCRATCH_FLAG_TMO = 15;
+
 // Per-solve scratch for two-stage reductions.  One Scratch per stream:
 // the last-CTA norm counter is not shared between concurrent launches.
 struct Scratch {
@@ -20,7 +24,7 @@ struct Scratch {
     unsigned *counter = nullptr;
     cplx *red = nullptr;     // reduced dot outputs
     double *scal = nullptr;  // device scalar slots
-    int *flags = nullptr;    // device flags
+    int *flags = nullptr;    // device flags (16); flags[SCRATCH_FLAG_TMO]: a bounded wait ran out
     bbjd_status init(int64_t n, int max_cols, int nvec);
     void release();
 };

@@ -1505,7 +1505,7 @@ int Engine::rebuild_W_cholqr(int keep) {
             for (int i = 0; i < keep; ++i) g[i + (size_t)j * keep] = i <= j ? C(R[i + (size_t)j * keep]) : mk(0, 0);
         if (cudaMemcpyAsync(Zdev, g.data(), sizeof(cplx) * keep * keep, cudaMemcpyHostToDevice, st)) return -1;
         T.begin(KC_RESTART, 32.0 * n * keep);
-        if (restart_gemm(n, keep, keep, W, ld, Zdev, keep, W, st, dflag + FL_TMO)) return -1;
+        if (restart_gemm(n, keep, keep, W, ld, Zdev, keep, W, st, S.flags + SCRATCH_FLAG_TMO)) return -1;
         T.end();
         bytes_dev += 32.0 * n * keep;
         if (sync()) return -1;      // g is reused by the next pass
@@ -1649,7 +1649,12 @@ bbjd_status Engine::run() {
         bytes_dev += abytes_r;
         if (s) return s;
         BBJD_CUDA_TRY(cudaMemcpyAsync(pin_d, dscal, sizeof(double) * 2, cudaMemcpyDeviceToHost, st));
+        BBJD_CUDA_TRY(cudaMemcpyAsync(pin_i + FL_TMO, S.flags + SCRATCH_FLAG_TMO, sizeof(int),
+                                      cudaMemcpyDeviceToHost, st));
         if ((s = sync())) return s;
+        // a kernel whose bounded wait for its staged tiles ran out (the
+        // fused CGS update, the restart GEMM): its results are not valid
+        if (pin_i[FL_TMO]) return res->status = BBJD_ERR_DEVICE_TIMEOUT;
         // a non-finite norm (NaN / Inf from an operator or the pencil) is a
         // breakdown: no later step could recover from it
         if (!(pin_d[SC_UNORM] >= 1e-300) || !std::isfinite(pin_d[SC_UNORM]) ||
@@ -1760,7 +1765,7 @@ bbjd_status Engine::run() {
             }
             const double gb = 16.0 * n * (double)(k + keep);
             T.begin(KC_RESTART, 3 * gb);
-            int *tmo = dflag + FL_TMO;
+            int *tmo = S.flags + SCRATCH_FLAG_TMO;
             if ((s = restart_gemm(n, (int)k, (int)keep, V, ld, Zdev, (int)k, V, st, tmo))) return s;
             if (mixed && (s = to_c64(n * keep, V, Vs, st))) return s;
             if ((s = restart_gemm(n, (int)k, (int)keep, AV, ld, Zdev, (int)k, AV, st, tmo))) return s;
@@ -1794,7 +1799,7 @@ bbjd_status Engine::run() {
                 std::vector<cplx> gh((size_t)2 * keep * keep);
                 BBJD_CUDA_TRY(cudaMemcpyAsync(gh.data(), gram_out, sizeof(cplx) * 2 * keep * keep,
                                               cudaMemcpyDeviceToHost, st));
-                BBJD_CUDA_TRY(cudaMemcpyAsync(pin_i + FL_TMO, dflag + FL_TMO, sizeof(int),
+                BBJD_CUDA_TRY(cudaMemcpyAsync(pin_i + FL_TMO, S.flags + SCRATCH_FLAG_TMO, sizeof(int),
                                               cudaMemcpyDeviceToHost, st));
                 if ((s = sync())) return s;
                 // a TMA-staged restart GEMM whose bounded wait ran out
