@@ -122,6 +122,7 @@ def assert_eigs_match(P, ev, evecs, ref, ref_resid=None, kappas=None):
     for j, (lam, x) in enumerate(zip(ev, np.asarray(evecs).T)):
         i = idx[j]
         kap = kappas[i] if kappas is not None else eig_condition(P, lam)
+        assert np.isfinite(kap), f"{lam}: no condition number cached for its oracle value {ref[i]}"
         r = unscaled_residual(P, lam, x)
         if ref_resid is not None:
             r += ref_resid[i]
