@@ -26,7 +26,7 @@ def _check_pairs(P, ev, evecs, g, tol=1e-10):
     nA, nB = sp.linalg.norm(A), sp.linalg.norm(B)
     for lam, x in zip(ev, evecs.T):
         r = A @ x - lam * (B @ x)
-        # normalised residual of the north-star acceptance test
+        # normalised residual: the acceptance test of the benchmark metric
         assert np.linalg.norm(r) / ((nA + abs(lam) * nB) * np.linalg.norm(x)) < tol
         # the reference test suite's unscaled measure (tests/test_bbjd.py:96-98)
         assert np.linalg.norm(r) / np.linalg.norm(x) < 1e-8
