@@ -1,6 +1,7 @@
 // Device-resident block-bordered (BBT) pencil and its preconditioners.
 #pragma once
 
+#include <mutex>
 #include <vector>
 
 #include "dense.cuh"
@@ -84,4 +85,19 @@ struct bbjd_precond {
     int *err = nullptr;              // device: singular pivot seen
     double factor_seconds = 0.0;
     double min_pivot = 0.0;
+    // The BCR solve captured as CUDA graphs, one per (r, x, stride, nrhs,
+    // stream) seen twice: a solve calls the preconditioner with the same
+    // buffers every outer iteration, and one graph launch replaces its ~35
+    // kernel launches.
+    struct Graph {
+        const void *r = nullptr;
+        void *x = nullptr;
+        int64_t stride = 0;
+        int nrhs = 0;
+        cudaStream_t st = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        int launches = 0;               // kernels in the graph
+    };
+    std::vector<Graph> graphs;
+    std::mutex graph_mu;
 };

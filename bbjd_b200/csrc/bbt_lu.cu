@@ -845,8 +845,8 @@ static bbjd_status precond_apply(const bbjd_precond *pc, const cplx *r, cplx *x,
     return BBJD_SUCCESS;
 }
 
-bbjd_status precond_solve(const bbjd_precond *pc, int nrhs, const cplx *r, cplx *x, int64_t stride,
-                          cudaStream_t st) {
+static bbjd_status precond_launch(const bbjd_precond *pc, int nrhs, const cplx *r, cplx *x, int64_t stride,
+                                  cudaStream_t st) {
     const bool c64 = pc->precision == BBJD_MIXED;
 #define BBJD_PC(BS)                                                                       \
     if (pc->b == BS) {                                                                    \
@@ -863,6 +863,67 @@ bbjd_status precond_solve(const bbjd_precond *pc, int nrhs, const cplx *r, cplx 
     BBJD_PC(32)
 #undef BBJD_PC
     return BBJD_ERR_INVALID;
+}
+
+// The BCR solve through a cached CUDA graph.  The first call with a given
+// (r, x, stride, nrhs, stream) launches the kernels directly and records
+// the key; the second captures them (stream capture, thread-local mode) and
+// every call from then on launches the instantiated graph.  Block Jacobi
+// (one or two kernels), the legacy default stream and a stream the caller
+// is already capturing take the direct launches.  The kernels and their
+// arguments are the same either way, so the results are.
+constexpr size_t PC_GRAPH_MAX = 64;
+bbjd_status precond_solve(const bbjd_precond *pc_in, int nrhs, const cplx *r, cplx *x, int64_t stride,
+                          cudaStream_t st) {
+    auto *pc = const_cast<bbjd_precond *>(pc_in);
+    if (pc->kind != BBJD_PC_BBT_LU || st == nullptr || st == cudaStreamLegacy || st == cudaStreamPerThread)
+        return precond_launch(pc, nrhs, r, x, stride, st);
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+        cudaGetLastError();
+        return precond_launch(pc, nrhs, r, x, stride, st);
+    }
+    std::lock_guard<std::mutex> lock(pc->graph_mu);
+    bbjd_precond::Graph *g = nullptr;
+    for (auto &e : pc->graphs)
+        if (e.r == r && e.x == x && e.stride == stride && e.nrhs == nrhs && e.st == st) g = &e;
+    if (g && g->exec) {
+        BBJD_CUDA_TRY(cudaGraphLaunch(g->exec, st));
+        count_launch(g->launches);
+        return BBJD_SUCCESS;
+    }
+    if (!g) {
+        if (pc->graphs.size() < PC_GRAPH_MAX) {
+            bbjd_precond::Graph e;
+            e.r = r; e.x = x; e.stride = stride; e.nrhs = nrhs; e.st = st;
+            pc->graphs.push_back(e);
+        }
+        return precond_launch(pc, nrhs, r, x, stride, st);
+    }
+    // second call with this key: capture the launches, instantiate, launch
+    const long long l0 = g_launches.load();
+    if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaGetLastError();
+        return precond_launch(pc, nrhs, r, x, stride, st);
+    }
+    const bbjd_status s = precond_launch(pc, nrhs, r, x, stride, st);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(st, &graph);
+    const long long nl = g_launches.load() - l0;
+    g_launches.fetch_sub(nl);            // captured, not launched
+    cudaGraphExec_t exec = nullptr;
+    const bool ok = s == BBJD_SUCCESS && e == cudaSuccess && graph &&
+                    cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+    if (graph) cudaGraphDestroy(graph);
+    if (!ok) {
+        cudaGetLastError();
+        return precond_launch(pc, nrhs, r, x, stride, st);
+    }
+    g->exec = exec;
+    g->launches = (int)nl;
+    BBJD_CUDA_TRY(cudaGraphLaunch(exec, st));
+    count_launch(g->launches);
+    return BBJD_SUCCESS;
 }
 
 double precond_bytes(const bbjd_precond *pc, int nrhs) {
@@ -1115,6 +1176,8 @@ extern "C" bbjd_status bbjd_precond_create(const bbjd_bbt_matrix *m, bbjd_zomple
 
 extern "C" void bbjd_precond_free(bbjd_precond *pc) {
     if (!pc) return;
+    for (auto &g : pc->graphs)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
     cudaFree(pc->pool);
     cudaFree(pc->pool32);
     cudaFree(pc->Y);
