@@ -668,13 +668,16 @@ __global__ void __launch_bounds__(256, 1) k_restart_gemm_tma(const __grid_consta
 
 // Gram stage 1: partial[g] (keep x keep, column-major) = X_g^H Y_g over the
 // CTA's row range.  Each thread holds a 5 x 5 tile (keep <= 80 per launch
-// tile; larger keep tiles over blockIdx.y / z).
-constexpr int GR_T = 80, GR_SUB = 16;
+// tile; larger keep tiles over blockIdx.y / z).  The 8-row slices of X and
+// Y are staged by cp.async into two buffers, so the next slice loads while
+// this one is multiplied; rows past the range and columns past keep are
+// zero-filled.
+constexpr int GR_T = 80, GR_SUB = 8;
 __global__ void __launch_bounds__(256) k_gram(int64_t n, int keep, const cplx *__restrict__ X,
                                               const cplx *__restrict__ Y, int64_t ldx,
                                               int64_t rpc, cplx *__restrict__ partial) {
-    __shared__ cplx sX[GR_SUB][GR_T];
-    __shared__ cplx sY[GR_SUB][GR_T];
+    __shared__ __align__(16) cplx sX[2][GR_SUB][GR_T];
+    __shared__ __align__(16) cplx sY[2][GR_SUB][GR_T];
     const int tid = threadIdx.x, ta = tid & 15, tb = tid >> 4;
     const int a0 = blockIdx.y * GR_T, b0 = blockIdx.z * GR_T;
     const int64_t r0 = (int64_t)blockIdx.x * rpc, r1 = min(n, r0 + rpc);
@@ -683,28 +686,43 @@ __global__ void __launch_bounds__(256) k_gram(int64_t n, int keep, const cplx *_
     for (int u = 0; u < 5; ++u)
 #pragma unroll
         for (int v = 0; v < 5; ++v) acc[u][v] = mk(0.0, 0.0);
-    for (int64_t rs = r0; rs < r1; rs += GR_SUB) {
+    // thread tid copies rows rr of columns c = e / GR_SUB, e = tid + 256 i:
+    // consecutive threads take consecutive rows of one column
+    auto stage = [&](int64_t rs, int buf) {
         for (int e = tid; e < GR_SUB * GR_T; e += 256) {
             const int c = e / GR_SUB, rr = e - c * GR_SUB;
             const int64_t row = rs + rr;
-            const bool ok = row < r1;
-            sX[rr][c] = (ok && a0 + c < keep) ? X[(int64_t)(a0 + c) * ldx + row] : mk(0.0, 0.0);
-            sY[rr][c] = (ok && b0 + c < keep) ? Y[(int64_t)(b0 + c) * ldx + row] : mk(0.0, 0.0);
+            const bool okx = row < r1 && a0 + c < keep;
+            const bool oky = row < r1 && b0 + c < keep;
+            cp_async16(&sX[buf][rr][c], X + (okx ? (int64_t)(a0 + c) * ldx + row : 0), okx ? 16 : 0);
+            cp_async16(&sY[buf][rr][c], Y + (oky ? (int64_t)(b0 + c) * ldx + row : 0), oky ? 16 : 0);
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    };
+    if (r0 < r1) stage(r0, 0);
+    int buf = 0;
+    for (int64_t rs = r0; rs < r1; rs += GR_SUB) {
+        if (rs + GR_SUB < r1) {
+            stage(rs + GR_SUB, buf ^ 1);       // the buffer the last slice used
+            asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+        } else {
+            asm volatile("cp.async.wait_group 0;\n" ::: "memory");
         }
         __syncthreads();
 #pragma unroll 4
         for (int rr = 0; rr < GR_SUB; ++rr) {
             cplx xv[5], yv[5];
 #pragma unroll
-            for (int u = 0; u < 5; ++u) xv[u] = sX[rr][ta + 16 * u];
+            for (int u = 0; u < 5; ++u) xv[u] = sX[buf][rr][ta + 16 * u];
 #pragma unroll
-            for (int v = 0; v < 5; ++v) yv[v] = sY[rr][tb + 16 * v];
+            for (int v = 0; v < 5; ++v) yv[v] = sY[buf][rr][tb + 16 * v];
 #pragma unroll
             for (int u = 0; u < 5; ++u)
 #pragma unroll
                 for (int v = 0; v < 5; ++v) cfmac(acc[u][v], xv[u], yv[v]);
         }
-        __syncthreads();
+        __syncthreads();                      // this buffer is free for the slice after next
+        buf ^= 1;
     }
     cplx *out = partial + (int64_t)blockIdx.x * keep * keep;
 #pragma unroll
