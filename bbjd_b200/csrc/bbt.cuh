@@ -82,6 +82,13 @@ struct bbjd_precond {
     bbjd::cplx *tau_part = nullptr;  // [G][2][t]
     bbjd::cplx *x2 = nullptr;        // [2][t]
     bbjd::cplx *gbuf = nullptr;      // [2][t] r2 - F1 y
+    // The reduced system of level `cut` (the first level with <= 64 blocks,
+    // mcut = N b unknowns) solved by its dense inverse instead of the levels
+    // below it and the top block: one matrix-vector product in place of a
+    // dozen dependent small-level kernels.
+    int64_t cut = -1, mcut = 0;
+    bbjd::cplx *Minv = nullptr;      // mcut x mcut column-major
+    bbjd::cplx *mpart = nullptr;     // [MV_CHUNKS][2][mcut] partial products
     int *err = nullptr;              // device: singular pivot seen
     double factor_seconds = 0.0;
     double min_pivot = 0.0;

@@ -497,6 +497,54 @@ __global__ void __launch_bounds__(256) k_bcr_bwd_cta(int64_t N, const T *__restr
     }
 }
 
+// The reduced system's dense inverse applied to R right-hand sides, in two
+// deterministic stages: part[c][q][i] = sum over the c-th chunk of columns j
+// of Minv[i, j] rhs[q][j] (a thread per row i, the column-major Minv read
+// coalesced), then x[q][i] = sum over c of part[c][q][i] in chunk order.
+constexpr int MV_CHUNKS = 48;
+template <int R>
+__global__ void __launch_bounds__(256) k_dense_mv(int64_t m, const cplx *__restrict__ M,
+                                                  const cplx *__restrict__ rhs, int64_t rs,
+                                                  cplx *__restrict__ part) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t cc = (m + gridDim.y - 1) / gridDim.y;
+    const int64_t j0 = (int64_t)blockIdx.y * cc, j1 = min(m, j0 + cc);
+    if (i >= m) return;
+    cplx acc[R];
+#pragma unroll
+    for (int q = 0; q < R; ++q) acc[q] = mk(0.0, 0.0);
+    for (int64_t j = j0; j < j1; ++j) {
+        const cplx a = ldg_stream(M + j * m + i);
+#pragma unroll
+        for (int q = 0; q < R; ++q) cfma(acc[q], a, __ldg(rhs + q * rs + j));
+    }
+#pragma unroll
+    for (int q = 0; q < R; ++q) part[((int64_t)blockIdx.y * R + q) * m + i] = acc[q];
+}
+
+template <int R>
+__global__ void __launch_bounds__(256) k_dense_mv_sum(int64_t m, int chunks, const cplx *__restrict__ part,
+                                                      cplx *__restrict__ x, int64_t xs) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= R * m) return;
+    const int q = (int)(e / m);
+    const int64_t i = e - q * m;
+    cplx s = mk(0.0, 0.0);
+    for (int c = 0; c < chunks; ++c) s = cadd(s, part[((int64_t)c * R + q) * m + i]);
+    x[q * xs + i] = s;
+}
+
+// Two right-hand sides of the reduced system at unit vectors: rhs[q] =
+// e_(i0 + q) (zero when i0 + q = m), stride rs.
+__global__ void k_unit_pair(int64_t m, int64_t i0, cplx *__restrict__ rhs, int64_t rs) {
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < 2 * m;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int q = (int)(e / m);
+        const int64_t j = e - q * m;
+        rhs[q * rs + j] = mk(j == i0 + q ? 1.0 : 0.0, 0.0);
+    }
+}
+
 // Block-Jacobi apply: x_j = Dinv_j r_j for every interior block.
 template <int BS, int R, typename T>
 __global__ void __launch_bounds__(256) k_bjac(int64_t nblk, const T *__restrict__ Dinv,
@@ -750,21 +798,27 @@ static const T *fac(const bbjd_precond *pc, const cplx *p64) {
 }
 
 // Solve K x = r for the interior with R right-hand sides (input stride rs,
-// output stride xs).  x may alias r.  T: factor element type.
+// output stride xs).  x may alias r.  T: factor element type.  From level
+// `start` > 0 the right-hand sides are already in that level's buffer and
+// the solution is left in its x buffer (the factorisation uses this to
+// form Minv).  With use_cut, the levels from pc->cut on and the top block
+// are replaced by the reduced system's dense inverse.
 template <int BS, int R, typename T = cplx>
 static bbjd_status bcr_solve(const bbjd_precond *pc, const cplx *r, int64_t rs, cplx *x, int64_t xs,
-                             cudaStream_t st) {
+                             cudaStream_t st, int64_t start = 0, bool use_cut = true) {
     // Vectors: level 0 is the caller's r / x; level l >= 1 and the top block
     // live in lvl_rhs / lvl_x at levels[l].vec_off / top_off, per-RHS stride
     // lvl_total.
     const int cap = 16 * num_sms();
     const int64_t L = (int64_t)pc->levels.size();
     const int64_t tot = pc->lvl_total;
+    const bool cut = use_cut && pc->Minv && pc->cut > start;
+    const int64_t stop = cut ? pc->cut : L;          // forward levels [start, stop)
     auto rhs_at = [&](int64_t l) -> const cplx * {
         return l == 0 ? r : (l < L ? pc->lvl_rhs + pc->levels[l].vec_off : pc->lvl_rhs + pc->top_off);
     };
     auto rstride = [&](int64_t l) -> int64_t { return l == 0 ? rs : tot; };
-    for (int64_t l = 0; l < L; ++l) {
+    for (int64_t l = start; l < stop; ++l) {
         const auto &lv = pc->levels[l];
         cplx *nxt = (l + 1 < L) ? pc->lvl_rhs + pc->levels[l + 1].vec_off : pc->lvl_rhs + pc->top_off;
         const T *Alpha = fac<T>(pc, lv.Alpha), *Beta = fac<T>(pc, lv.Beta);
@@ -775,11 +829,21 @@ static bbjd_status bcr_solve(const bbjd_precond *pc, const cplx *r, int64_t rs, 
         }
         BBJD_LAUNCH_CHECK();
     }
-    cplx *tx = L ? pc->lvl_x + pc->top_off : x;
-    const int64_t txs = L ? tot : xs;
-    k_bcr_top<BS, R, T><<<1, 32, 0, st>>>(fac<T>(pc, pc->Dinv_top), rhs_at(L), rstride(L), tx, txs);
-    BBJD_LAUNCH_CHECK();
-    for (int64_t l = L - 1; l >= 0; --l) {
+    if (cut) {
+        const int64_t m = pc->mcut;
+        cplx *xc = pc->lvl_x + pc->levels[pc->cut].vec_off;
+        k_dense_mv<R><<<dim3((unsigned)((m + 255) / 256), MV_CHUNKS), 256, 0, st>>>(
+            m, pc->Minv, rhs_at(pc->cut), tot, pc->mpart);
+        BBJD_LAUNCH_CHECK();
+        k_dense_mv_sum<R><<<(unsigned)((R * m + 255) / 256), 256, 0, st>>>(m, MV_CHUNKS, pc->mpart, xc, tot);
+        BBJD_LAUNCH_CHECK();
+    } else {
+        cplx *tx = L ? pc->lvl_x + pc->top_off : x;
+        const int64_t txs = L ? tot : xs;
+        k_bcr_top<BS, R, T><<<1, 32, 0, st>>>(fac<T>(pc, pc->Dinv_top), rhs_at(L), rstride(L), tx, txs);
+        BBJD_LAUNCH_CHECK();
+    }
+    for (int64_t l = stop - 1; l >= start; --l) {
         const auto &lv = pc->levels[l];
         const cplx *xup = (l + 1 < L) ? pc->lvl_x + pc->levels[l + 1].vec_off : pc->lvl_x + pc->top_off;
         cplx *xo = l == 0 ? x : pc->lvl_x + lv.vec_off;
@@ -940,7 +1004,18 @@ double precond_bytes(const bbjd_precond *pc, int nrhs) {
         // forward: read 3 rhs blocks per even, write 1; backward: read rhs + 2 x, write 1
         bytes += 16.0 * nrhs * pc->b * (4.0 * lv.n_even + 4.0 * lv.n_odd + 2.0 * lv.n_even);
     }
-    bytes += bb;  // top
+    if (pc->Minv) {
+        // the levels from `cut` on and the top block are replaced by the
+        // dense inverse (read once) and its partial products
+        for (size_t l = (size_t)pc->cut; l < pc->levels.size(); ++l) {
+            const auto &lv = pc->levels[l];
+            bytes -= bb * (3.0 * lv.n_odd + 2.0 * lv.n_even);
+            bytes -= 16.0 * nrhs * pc->b * (4.0 * lv.n_even + 4.0 * lv.n_odd + 2.0 * lv.n_even);
+        }
+        bytes += 16.0 * (double)pc->mcut * pc->mcut + 16.0 * nrhs * pc->mcut * (2.0 * MV_CHUNKS + 2.0);
+    } else {
+        bytes += bb;  // top
+    }
     if (pc->t > 0) {
         bytes += es * (double)pc->nb * pc->t * 2.0;          // F1 and Y
         bytes += 16.0 * nrhs * (double)pc->nb * 3.0;         // y read twice, x1 written
@@ -1025,6 +1100,43 @@ static bbjd_status factor_bcr(bbjd_precond *pc, const bbjd_bbt_matrix *m, cplx s
     int err = 0;
     BBJD_CUDA_TRY(cudaMemcpy(&err, pc->err, sizeof(int), cudaMemcpyDeviceToHost));
     if (err) return BBJD_ERR_BREAKDOWN;
+
+    // dense inverse of the reduced system at the first level with <= 64
+    // blocks (levels from there on and the top block are ~13 dependent
+    // latency-bound launches per solve): column pairs by sub-solves from
+    // that level on unit right-hand sides
+    pc->cut = -1;
+    for (int64_t l = 1; l < (int64_t)pc->levels.size(); ++l)
+        if (pc->levels[l].N <= 64) {
+            pc->cut = l;
+            break;
+        }
+    if (pc->cut > 0) {
+        // only where the inverse is a small part of what a solve reads (large
+        // pencils: 63 MB against 2.6 GB of factors at 31,250 blocks of 32)
+        double factor_bytes = 0.0;
+        for (const auto &lv : pc->levels) factor_bytes += 16.0 * BB * (3.0 * lv.n_odd + 2.0 * lv.n_even);
+        const double m = (double)(pc->levels[pc->cut].N * BS);
+        if (16.0 * m * m > 0.05 * factor_bytes) pc->cut = -1;
+    }
+    if (pc->cut > 0) {
+        const int64_t m = pc->levels[pc->cut].N * BS, tot = pc->lvl_total;
+        pc->mcut = m;
+        BBJD_CUDA_TRY(cudaMalloc(&pc->Minv, sizeof(cplx) * (size_t)m * m));
+        BBJD_CUDA_TRY(cudaMalloc(&pc->mpart, sizeof(cplx) * (size_t)MV_CHUNKS * 2 * m));
+        cplx *rc = pc->lvl_rhs + pc->levels[pc->cut].vec_off;
+        const cplx *xc = pc->lvl_x + pc->levels[pc->cut].vec_off;
+        for (int64_t i0 = 0; i0 < m; i0 += 2) {
+            k_unit_pair<<<grid_for(2 * m, 256, cap), 256, 0, st>>>(m, i0, rc, tot);
+            BBJD_LAUNCH_CHECK();
+            bbjd_status s = bcr_solve<BS, 2>(pc, nullptr, 0, nullptr, 0, st, pc->cut, false);
+            if (s != BBJD_SUCCESS) return s;
+            BBJD_CUDA_TRY(cudaMemcpy2DAsync(pc->Minv + i0 * m, sizeof(cplx) * m, xc, sizeof(cplx) * tot,
+                                            sizeof(cplx) * m, (size_t)std::min<int64_t>(2, m - i0),
+                                            cudaMemcpyDeviceToDevice, st));
+        }
+        BBJD_CUDA_TRY(cudaStreamSynchronize(st));
+    }
     if (pc->t == 0) return BBJD_SUCCESS;
 
     // border: Y = K^-1 E (t right-hand sides, two at a time), S = G - F1 Y
@@ -1190,6 +1302,8 @@ extern "C" void bbjd_precond_free(bbjd_precond *pc) {
     cudaFree(pc->tau_part);
     cudaFree(pc->x2);
     cudaFree(pc->gbuf);
+    cudaFree(pc->Minv);
+    cudaFree(pc->mpart);
     cudaFree(pc->err);
     delete pc;
 }

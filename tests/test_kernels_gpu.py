@@ -107,6 +107,35 @@ def test_bbt_lu_graph_replay_matches_direct_launches(precision):
     pc.close()
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_bbt_lu_full_size_backward_error(precision):
+    """The benchmark's n = 1,000,064 pencil, whose BCR solve replaces its
+    levels below 64 blocks and the top block by the reduced system's dense
+    inverse: the 2-RHS solve's backward error, computed on the host with
+    the numpy block product, is at the FP64 level (complex64 level for the
+    mixed factors)."""
+    import torch
+    P = make_pencil(32, 31250, 64, seed=0)
+    sigma = 3.0
+    dev = DevicePencil(P)
+    pc = DevicePreconditioner(dev, sigma, "exact", precision=precision)
+    r = np.stack([_rand(P.n, 21), _rand(P.n, 22)])
+    rd = _dev(r)
+    xd = torch.empty_like(rd)
+    lib = _lib.load()
+    assert lib.bbjd_precond_solve(pc.handle, 2, rd.data_ptr(), xd.data_ptr(), None) == 0
+    torch.cuda.synchronize()
+    x = _host(xd)
+    nA = np.sqrt(sum(np.vdot(a, a).real for a in (P.Ad, P.Al, P.Au, P.E, P.F)))
+    nB = np.sqrt(np.vdot(P.Bd, P.Bd).real)
+    bound = 1e-13 if precision == "fp64" else 1e-5
+    for q in range(2):
+        res = P.matvec_A(x[q]) - sigma * P.matvec_B(x[q]) - r[q]
+        assert np.linalg.norm(res) / ((nA + abs(sigma) * nB) * np.linalg.norm(x[q])) < bound
+    pc.close()
+    dev.close()
+
+
 def test_bbt_lu_in_place():
     import torch
     P = make_pencil(16, 50, 8, seed=1)
