@@ -94,8 +94,8 @@ struct bbjd_precond {
     double min_pivot = 0.0;
     // The BCR solve captured as CUDA graphs, one per (r, x, stride, nrhs,
     // stream) seen twice: a solve calls the preconditioner with the same
-    // buffers every outer iteration, and one graph launch replaces its ~35
-    // kernel launches.
+    // buffers every outer iteration, and one graph launch replaces its
+    // ~24 kernel launches.
     struct Graph {
         const void *r = nullptr;
         void *x = nullptr;
