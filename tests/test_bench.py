@@ -47,3 +47,22 @@ def test_reference_run_record_counts_distinct_pairs():
     assert rec["iters"] >= 200 and len(rec["time"]) >= 200
     assert 1 <= rec["pairs"] <= rec["returned"]
     assert np.all(np.diff(rec["time"]) >= 0)
+
+
+def test_reference_arm_reports_unavailable_without_its_cached_run(monkeypatch, capsys):
+    import json
+    import types
+    monkeypatch.setattr(bench, "REF_RUN", "/nonexistent/bbt_n1000064.npz")
+    monkeypatch.delenv("RANK", raising=False)
+    args = types.SimpleNamespace(warmup=3, steps=1, ref_iters=16)
+    assert bench.run_reference(args) == 0
+    line = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and "unavailable" in line
+
+
+def test_reference_arm_other_ranks_do_nothing(monkeypatch, capsys):
+    import types
+    monkeypatch.setenv("RANK", "1")
+    monkeypatch.setenv("WORLD_SIZE", "2")
+    assert bench.run_reference(types.SimpleNamespace(warmup=3, steps=1, ref_iters=16)) == 0
+    assert capsys.readouterr().out == ""
